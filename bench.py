@@ -1,0 +1,393 @@
+"""Benchmark: batched greedy cosine, pairs/s, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): greedy cosine over every pair of 100k reference x 100k
+query spectra (1e10 pairs) with lognormal peak counts (median 60, sigma 1.0,
+clipped to [5, 1000]), m/z U(50, 2000) float32, intensities Exp(1) scaled to
+max 1, tolerance 0.01, mz_power 0, intensity_power 1, match_limit 4096;
+seeded synthetic data (the reference benchmarks on GNPS, which is not
+available offline).  Dense outputs (score f32, matches i32, overflow u8 per
+pair) are written to device buffers reused across row blocks.  Inputs are
+larger than L2 (no flush needed).
+
+Reported (one JSON line, rank 0):
+  value       pairs/s with inputs resident in HBM (device time, max over ranks)
+  e2e         pairs/s through the public API (CudaCosineGreedy.matrix,
+              array_type="sparse") from host spectra, H2D + D2H included
+  plain       pairs/s of the one-pair-per-thread kernel on a row sample
+  roofline    join kernel: algorithmic bytes / its live CUDA-event duration
+              vs measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C restatement, all host threads) on a row
+              sample of the same workload (rank 0, N=1 only)
+Multi-GPU (torchrun): each rank computes its own 100k-reference shard against
+the same queries; no collective on the data path ("scaling": "weak").
+
+--impl reference times the reference's CPU implementation of the path: the
+reference is a Python/Numba package whose GPU kernel cannot be built here,
+so its CPU restatement (oracle/, C + OpenMP, every host thread) stands in,
+on row samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cosine-similarity_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cosine-greedy pairs/s (batched, 1 B200, |err|<=1e-5)"
+UNIT = "pairs/s"
+TOL, MATCH_LIMIT, N_MAX_PEAKS = 0.01, 4096, 1024
+WORKLOAD = ("batched greedy cosine 100k x 100k, lognormal peaks (median 60, sigma 1.0, "
+            "clip 5-1000), m/z U(50,2000), tol 0.01, powers (0,1), match_limit 4096")
+BYTES_PER_PAIR = 9
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=100_000, help="spectra per side (default 100k)")
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--plain-rows", type=int, default=0, help="rows for the plain sample (0=auto)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--config", type=str, default="", help="JSON cms_cosine_config override")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_data(args, rank):
+    from cudams import synthetic
+
+    ref = synthetic.lognormal_spectra(args.n, seed=args.seed + 1000 * (rank + 1))
+    qry = synthetic.lognormal_spectra(args.n, seed=args.seed)
+    return ref, qry
+
+
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+def cpu_baseline(ref, qry, seconds: float):
+    """CPU oracle on a row sample of the workload, all host threads."""
+    from oracle import oracle
+
+    threads = oracle.available_threads()
+    rows = 4
+    while True:
+        sub = ref.subset(0, rows)
+        t = time.perf_counter()
+        oracle.cosine_greedy(sub, qry, TOL, 0.0, MATCH_LIMIT, threads=threads)
+        dt = time.perf_counter() - t
+        if dt >= seconds / 4 or rows >= ref.n:
+            break
+        rows = min(ref.n, max(rows * 2, int(rows * (seconds / 4) / max(dt, 1e-3))))
+    rate = rows * qry.n / dt
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{rows} reference rows x {qry.n} queries ({rows * qry.n} pairs), "
+                      f"{dt:.1f} s, C restatement (oracle/) with OpenMP"}
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    ref, qry = make_data(args, 0)
+    from oracle import oracle
+
+    threads = oracle.available_threads()
+    # size one step to ~args.cpu_seconds / (steps + warmup) of CPU work
+    probe_rows = 4
+    t = time.perf_counter()
+    oracle.cosine_greedy(ref.subset(0, probe_rows), qry, TOL, 0.0, MATCH_LIMIT, threads=threads)
+    per_row = (time.perf_counter() - t) / probe_rows
+    budget = max(2.0, 120.0 / max(1, args.steps + args.warmup))
+    rows = max(1, min(ref.n, int(budget / max(per_row, 1e-6))))
+    for w in range(args.warmup):
+        oracle.cosine_greedy(ref.subset(w * rows % ref.n, min(ref.n, w * rows % ref.n + 1)), qry,
+                             TOL, 0.0, MATCH_LIMIT, threads=threads)
+    times = []
+    for k in range(args.steps):
+        r0 = (k * rows) % max(1, ref.n - rows + 1)
+        t = time.perf_counter()
+        oracle.cosine_greedy(ref.subset(r0, r0 + rows), qry, TOL, 0.0, MATCH_LIMIT,
+                             threads=threads)
+        times.append(time.perf_counter() - t)
+    total = sum(times)
+    rate = rows * qry.n * args.steps / total
+    sample = (f"{rows} reference rows x {qry.n} queries per step, C restatement of the "
+              f"reference algorithm (oracle/, OpenMP, {threads} threads)")
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "n_ref": args.n, "n_query": args.n},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from cudams import _native, kernels
+    from cudams.similarity import CudaCosineGreedy
+
+    dev = _native.require_cuda(local)
+    torch.cuda.set_device(dev)
+    ref, qry = make_data(args, rank)
+    cfg = json.loads(args.config) if args.config else None
+    if cfg is None:
+        from cudams import autotune
+
+        cfg = autotune.choose_config(ref, qry, TOL)
+    rd, qd = ref.to_device(dev), qry.to_device(dev)
+    R, Q = ref.n, qry.n
+    free, _ = torch.cuda.mem_get_info(dev)
+    rows = int(min(R, max(1024, (min(free * 0.6, 48e9)) // (Q * BYTES_PER_PAIR))))
+    blocks = [(r0, min(R, r0 + rows)) for r0 in range(0, R, rows)]
+    sub = [ref.subset(a, b).to_device(dev) if (a, b) != (0, R) else rd for a, b in blocks]
+    out = (torch.empty((rows, Q), dtype=torch.float32, device=dev),
+           torch.empty((rows, Q), dtype=torch.int32, device=dev),
+           torch.empty((rows, Q), dtype=torch.uint8, device=dev))
+    stream = torch.cuda.current_stream(dev)
+    ctx = _native.context(dev.index)
+
+    def step():
+        for (a, b), s in zip(blocks, sub):
+            o = tuple(t[: b - a] for t in out)
+            kernels.cosine_greedy_dense(s, qd, TOL, 0.0, MATCH_LIMIT, out=o, config=cfg,
+                                        stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    bits = ctx.take_device_error(_native.stream_handle(stream))
+    if bits:
+        raise RuntimeError(f"device error word {bits} during warm-up")
+    ctx.profile_read(reset=True)
+    ctx.profile_enable(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    stage_ms, stage_n = ctx.profile_read(reset=True)
+    ctx.profile_enable(False)
+    ms_max = max_over_ranks(ms, world)
+    pairs_rank = R * Q * args.steps
+    value = pairs_rank * world / (ms_max / 1000.0)
+
+    # roofline of the dominant kernel (join: HBM-write bound dense output)
+    names = _native.PROFILE_STAGE_NAMES
+    dom = int(np.argmax(stage_ms))
+    join_launches = max(1, int(stage_n[3]))
+    join_ms = stage_ms[3] / join_launches
+    pairs_per_launch = R * Q * args.steps / join_launches
+    peaks_bytes = 12 * (ref.n_peaks / len(blocks) + qry.n_peaks)
+    alg_bytes = BYTES_PER_PAIR * pairs_per_launch + peaks_bytes
+    hbm, peak_kind = measured_peaks()
+    achieved = alg_bytes / (join_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": "join_kernel", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs (copy)",
+                "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": join_ms,
+                "stage_ms_per_step": {n: float(v) / args.steps for n, v in zip(names, stage_ms)},
+                "dominant_stage": names[dom]}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded; stands in for GNPS)",
+            "config": {"workload": WORKLOAD, "n_ref_per_rank": R, "n_query": Q,
+                       "pairs_per_step_per_rank": R * Q, "row_blocks": len(blocks),
+                       "tuning": cfg, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"row shards x{world}, no collective"},
+            "gpu_launches": int(stage_n.sum()),
+            "roofline": roofline, "clocks": clocks.summary()}
+
+    # plain comparator (same inputs, row sample)
+    if not args.no_plain:
+        prow = args.plain_rows or max(256, min(R, 2048))
+        psub = ref.subset(0, prow).to_device(dev)
+        pout = tuple(t[:prow] for t in out)
+        kernels.cosine_greedy_plain(psub, qd, TOL, 0.0, MATCH_LIMIT, N_MAX_PEAKS, out=pout)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        kernels.cosine_greedy_plain(psub, qd, TOL, 0.0, MATCH_LIMIT, N_MAX_PEAKS, out=pout)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain_rate = prow * Q / (pms / 1000.0)
+        line["plain"] = {"value": plain_rate, "unit": UNIT,
+                         "sample": f"{prow} reference rows x {Q} queries, one launch"}
+        line["speedup_vs_plain"] = value / world / plain_rate
+
+    # end to end through the public API from host spectra
+    if not args.no_e2e:
+        k = CudaCosineGreedy(tolerance=TOL, match_limit=MATCH_LIMIT, n_max_peaks=N_MAX_PEAKS,
+                             sparse_threshold=0.75, config=cfg)
+        h2d = ref.host_bytes() + qry.host_bytes()
+        times, hits = [], 0
+        for i in range(1 + max(1, min(args.steps, 2))):
+            ref._device.clear()
+            qry._device.clear()
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            sp = k.matrix(ref, qry, array_type="sparse")
+            torch.cuda.synchronize()
+            if i > 0:
+                times.append(time.perf_counter() - t)
+            hits = sp.row.shape[0] if hasattr(sp, "row") else 0
+        e2e_s = max_over_ranks(statistics.median(times), world)
+        e2e = R * Q * world / e2e_s
+        line["e2e"] = {"value": e2e, "unit": UNIT,
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(hits * 17 + 8),
+                       "path": "CudaCosineGreedy.matrix(array_type='sparse', threshold 0.75)",
+                       "hits": int(hits)}
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(ref, qry, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,125 @@
+// Internal declarations shared by the CUDA translation units of
+// libcudams_b200.so.  Public entry points live in include/cudams_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+#include <utility>
+#include <vector>
+
+#include "../../include/cudams_b200.h"
+
+namespace cms {
+
+// Device error word bits (cms_take_device_error).
+enum : uint32_t {
+    kErrSpectrumTooLong = 1u << 0,  // a spectrum exceeds CMS_MAX_PEAKS peaks
+    kErrSpillOverrun = 1u << 1,     // sparse spill list capacity exceeded
+    kErrBadOffsets = 1u << 2,       // offsets not non-decreasing / out of range
+};
+
+// One CSR spectrum set on the device (see the header comment of the public API).
+struct SpecSet {
+    const float* mz;
+    const double* a;  // nullptr => 1.0
+    const double* b;
+    const int64_t* off;
+    int64_t n;
+    int64_t n_peaks;
+};
+
+struct CosineArgs {
+    SpecSet ref;
+    SpecSet qry;
+    double tol;
+    double shift;
+    int match_limit;
+};
+
+struct DenseOut {
+    float* score;
+    int32_t* matches;
+    uint8_t* overflow;
+    int64_t ld;
+};
+
+struct SparseOut {
+    int32_t* r;
+    int32_t* q;
+    float* score;
+    int32_t* matches;
+    uint8_t* overflow;
+    int64_t capacity;
+    unsigned long long* count;  // int64 count, as an atomically updatable word
+    float threshold;
+};
+
+// Thread-local last-error string.
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+
+// Growable device arena owned by a context (never shrinks until destroy).
+struct Arena {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace cms
+
+struct cms_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    cms::Arena scratch;       // per-call scratch (indices, lists, counters)
+    uint32_t* err_word = nullptr;  // device, 1 word
+    // profiling (cms_profile_*)
+    bool profile = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
+    std::vector<cudaEvent_t> event_pool;
+    int64_t launches[CMS_PROFILE_STAGES] = {0, 0, 0, 0, 0};
+};
+
+namespace cms {
+
+// Ensure the arena holds at least `bytes`; returns CMS_OK or an error code.
+int arena_reserve(cms_ctx* ctx, Arena& a, size_t bytes, cudaStream_t s);
+
+// Bump allocator over an arena region (256-byte aligned slices).
+struct Bump {
+    char* base;
+    size_t used;
+    size_t cap;
+    template <typename T>
+    T* take(size_t count) {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + count * sizeof(T);
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+inline size_t bump_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+bool check_specset(const SpecSet& s, const char* name);
+
+// Scope that counts `n` launches for a profiling stage and, when profiling
+// is on, records an event pair around them on stream `s`.
+class StageScope {
+  public:
+    StageScope(cms_ctx* ctx, int stage, int n, cudaStream_t s);
+    ~StageScope();
+
+  private:
+    cms_ctx* ctx_;
+    int stage_;
+    cudaStream_t s_;
+    cudaEvent_t stop_ = nullptr;
+};
+
+}  // namespace cms
+
+#define CMS_CUDA_TRY(expr)                                         \
+    do {                                                           \
+        cudaError_t _e = (expr);                                   \
+        if (_e != cudaSuccess) return cms::cuda_fail(_e, #expr);   \
+    } while (0)

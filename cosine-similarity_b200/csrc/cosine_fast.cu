@@ -1,0 +1,1127 @@
+// Tiled greedy cosine for sm_100a: cms_cosine_greedy / cms_cosine_greedy_sparse.
+//
+// Replaces the reference's per-pair Numba kernel (cudams/similarity/
+// spectrum_similarity_functions.py:39-262) and the batch loop around it
+// (cudams/similarity/CudaCosineGreedy.py:138-226).  Results are identical to
+// the plain kernel and to the oracle; only the way candidates are found and
+// ordered differs.
+//
+// Pipeline of one call (all on one stream, no host synchronisation):
+//   1. validate_kernel   offsets sane, spectra <= CMS_MAX_PEAKS; else every
+//                        later kernel exits at once and the error word is set
+//   2. norms_kernel      sqrt(sum (a*b)^2) per spectrum, sequential float64
+//   3. order kernels     reference spectra ordered by peak count, largest
+//                        first (log2 length classes), for load balance
+//   4. index kernels     query spectra are cut into tiles of tile_spectra;
+//                        each tile's peaks are bucketed by m/z (bucket width
+//                        >= 2*tol, buckets hashed modulo n_buckets) into a
+//                        CSR "tile stream" of (m/z, query<<16 | peak)
+//   5. join_kernel       persistent warps; one work item = (reference
+//                        spectrum, query tile).  Lanes take reference peaks,
+//                        jump through the bucket table to the tile-stream
+//                        entries inside the tolerance window (the
+//                        two-pointer sweep of the reference, with the second
+//                        pointer advanced by the index instead of one step at
+//                        a time), test them exactly in float64 and push
+//                        candidates into a per-warp shared-memory pool.  The
+//                        pool is sorted by query, each query's short
+//                        candidate run is resolved greedily by one lane, and
+//                        the row segment is written coalesced.  Pairs with
+//                        long runs (or >= match_limit candidates) are
+//                        appended to a spill list.
+//   6. pair_kernel       one CTA per spilled pair (or per pair of the whole
+//                        matrix in mode 2): exact generation-order sweep with
+//                        match_limit truncation, bitonic sort of (key, gen)
+//                        in shared memory, warp-parallel greedy with
+//                        used-peak bitmasks.
+#include <algorithm>
+#include <cmath>
+
+#include "cms_internal.cuh"
+
+namespace cms {
+namespace {
+
+constexpr int kJoinWarps = 8;
+constexpr int kJoinThreads = kJoinWarps * 32;
+constexpr int kPool = 256;        // candidate pool entries per warp
+constexpr int kSmallRun = 16;     // longer runs go to the pair kernel
+constexpr int kMaxTile = 4096;    // max query spectra per tile (hasbits size)
+constexpr int kOrderClasses = 17; // log2 length classes (0..16)
+
+__device__ __forceinline__ double peak_a(const double* a, int64_t i) { return a ? a[i] : 1.0; }
+
+// ---------------------------------------------------------------------------
+// 1. validation
+// ---------------------------------------------------------------------------
+__global__ void validate_kernel(SpecSet S, uint32_t* bad, uint32_t* err) {
+    const int64_t n = S.n;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lo = S.off[s], hi = S.off[s + 1];
+        uint32_t e = 0;
+        if (lo < 0 || hi < lo || hi > S.n_peaks) e |= kErrBadOffsets;
+        if (hi - lo > CMS_MAX_PEAKS) e |= kErrSpectrumTooLong;
+        if (e) {
+            atomicOr(err, e);
+            atomicOr(bad, 1u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. norms: sn[s] = sqrt(sum_k (a_k*b_k)^2), summed in peak order
+// ---------------------------------------------------------------------------
+__global__ void norms_kernel(SpecSet S, double* sn, const uint32_t* bad) {
+    if (*bad) return;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < S.n;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lo = S.off[s], hi = S.off[s + 1];
+        double acc = 0.0;
+        for (int64_t k = lo; k < hi; ++k) {
+            const double w = __dmul_rn(peak_a(S.a, k), S.b[k]);
+            acc = __dadd_rn(acc, __dmul_rn(w, w));
+        }
+        sn[s] = sqrt(acc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. reference order: largest length class first
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int length_class(int64_t len) {
+    return len <= 0 ? 0 : min(kOrderClasses - 1, 64 - __clzll((unsigned long long)len));
+}
+
+__global__ void order_count_kernel(SpecSet S, uint32_t* cls_count, const uint32_t* bad) {
+    if (*bad) return;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < S.n;
+         s += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cls_count[length_class(S.off[s + 1] - S.off[s])], 1u);
+}
+
+__global__ void order_scatter_kernel(SpecSet S, const uint32_t* cls_count, uint32_t* cls_cursor,
+                                     int32_t* order, const uint32_t* bad) {
+    if (*bad) return;
+    __shared__ uint32_t base[kOrderClasses];
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int c = kOrderClasses - 1; c >= 0; --c) {
+            base[c] = acc;
+            acc += cls_count[c];
+        }
+    }
+    __syncthreads();
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < S.n;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int c = length_class(S.off[s + 1] - S.off[s]);
+        const uint32_t pos = base[c] + atomicAdd(&cls_cursor[c], 1u);
+        order[pos] = (int32_t)s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. tile index over the query side
+// ---------------------------------------------------------------------------
+struct IndexGeom {
+    int tile;        // query spectra per tile
+    int n_tiles;
+    int nb;          // buckets per tile (power of two)
+    double inv_w;    // 1 / bucket width
+};
+
+__device__ __forceinline__ long long bucket_of(double x, double inv_w) {
+    return (long long)floor(x * inv_w);
+}
+
+// warp per spectrum: histogram of (tile, bucket)
+__global__ void index_count_kernel(SpecSet B, IndexGeom g, uint32_t* cnt, const uint32_t* bad) {
+    if (*bad) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned mask = (unsigned)(g.nb - 1);
+    for (int64_t s = warp; s < B.n; s += nwarps) {
+        const int64_t t = s / g.tile;
+        const int64_t lo = B.off[s], hi = B.off[s + 1];
+        uint32_t* c = cnt + t * (int64_t)g.nb;
+        for (int64_t k = lo + lane; k < hi; k += 32) {
+            const unsigned bk = (unsigned)bucket_of((double)B.mz[k], g.inv_w) & mask;
+            atomicAdd(&c[bk], 1u);
+        }
+    }
+}
+
+// CTA per tile: exclusive scan of the bucket counts into tab[t][0..nb], and
+// reset the counters to the bucket starts (scatter cursors).
+__global__ void index_scan_kernel(IndexGeom g, uint32_t* cnt_cur, uint32_t* tab,
+                                  const uint32_t* bad) {
+    if (*bad) return;
+    const int t = blockIdx.x;
+    uint32_t* c = cnt_cur + (int64_t)t * g.nb;
+    uint32_t* out = tab + (int64_t)t * (g.nb + 1);
+    const int per = (g.nb + blockDim.x - 1) / blockDim.x;
+    const int begin = min(g.nb, (int)threadIdx.x * per);
+    const int end = min(g.nb, begin + per);
+    uint32_t local = 0;
+    for (int k = begin; k < end; ++k) local += c[k];
+    // block exclusive scan of `local`
+    __shared__ uint32_t warp_sums[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = local;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t v = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v += u;
+        }
+        if (lane < nw) warp_sums[lane] = v;
+    }
+    __syncthreads();
+    uint32_t run = incl - local + (wid > 0 ? warp_sums[wid - 1] : 0u);
+    for (int k = begin; k < end; ++k) {
+        const uint32_t v = c[k];
+        out[k] = run;
+        c[k] = run;
+        run += v;
+    }
+    if (threadIdx.x == blockDim.x - 1) out[g.nb] = run;
+}
+
+// warp per spectrum: scatter (m/z, q_local<<16 | peak) into the tile stream
+__global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, uint2* ent,
+                                     const uint32_t* bad) {
+    if (*bad) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned mask = (unsigned)(g.nb - 1);
+    for (int64_t s = warp; s < B.n; s += nwarps) {
+        const int64_t t = s / g.tile;
+        const int64_t base = B.off[t * g.tile];
+        const uint32_t ql = (uint32_t)(s - t * g.tile);
+        const int64_t lo = B.off[s], hi = B.off[s + 1];
+        uint32_t* c = cur + t * (int64_t)g.nb;
+        for (int64_t k = lo + lane; k < hi; k += 32) {
+            const float mz = B.mz[k];
+            const unsigned bk = (unsigned)bucket_of((double)mz, g.inv_w) & mask;
+            const uint32_t pos = atomicAdd(&c[bk], 1u);
+            ent[base + pos] = make_uint2(__float_as_uint(mz), (ql << 16) | (uint32_t)(k - lo));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// shared helpers for greedy resolution
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long order_key(double k) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(k);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double key_from_order(unsigned long long o) {
+    const unsigned long long u = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+    return __longlong_as_double((long long)u);
+}
+// (key, gen) strictly precedes (key', gen') in the greedy order
+__device__ __forceinline__ bool before(double k1, uint32_t g1, double k2, uint32_t g2) {
+    return k1 > k2 || (k1 == k2 && g1 > g2);
+}
+
+struct SpillList {
+    int2* pairs;  // (reference, query)
+    unsigned int* count;
+    unsigned int cap;
+};
+
+__device__ __forceinline__ void spill_push(const SpillList& sl, int r, int q, uint32_t* err) {
+    const unsigned int pos = atomicAdd(sl.count, 1u);
+    if (pos < sl.cap)
+        sl.pairs[pos] = make_int2(r, q);
+    else
+        atomicOr(err, kErrSpillOverrun);
+}
+
+// ---------------------------------------------------------------------------
+// 5. join kernel
+// ---------------------------------------------------------------------------
+struct JoinParams {
+    SpecSet A;  // sweeping side (one spectrum per work item)
+    SpecSet B;  // indexed side (tiles)
+    const double* snA;
+    const double* snB;
+    const int32_t* a_order;
+    const uint32_t* tab;
+    const uint2* ent;
+    IndexGeom g;
+    double tol;
+    double shift;
+    int match_limit;
+    int widen;  // bucket range widened by one on each side
+    float init_width_scale;  // initial sub-range width = clamp(scale / n_a_peaks)
+    unsigned long long* work;
+    SpillList spill;
+    DenseOut dense;
+    SparseOut sparse;
+    uint32_t* err;
+    const uint32_t* bad;
+};
+
+struct WarpSmem {
+    double key[kPool];
+    uint32_t gen[kPool];
+    uint32_t sk[kPool];           // (q_rel << 16) | slot, sorted
+    uint16_t run_start[kPool + 1];
+    float res_score[kPool];
+    int32_t res_matches[kPool];
+    uint32_t hasbits[kMaxTile / 32];
+    int n;
+    int n_runs;
+};
+
+// bitonic sort of s[0..m) ascending, m a power of two, by one warp
+__device__ void warp_bitonic_u32(uint32_t* s, int m, int lane) {
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < m; i += 32) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const uint32_t x = s[i], y = s[ixj];
+                    const bool up = (i & k) == 0;
+                    if (up ? (x > y) : (x < y)) {
+                        s[i] = y;
+                        s[ixj] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+template <bool A_IS_REF, bool SPARSE>
+__global__ void __launch_bounds__(kJoinThreads)
+join_kernel(JoinParams P) {
+    if (*P.bad) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const int64_t nA = P.A.n;
+    const int64_t n_items = nA * (int64_t)P.g.n_tiles;
+    const unsigned nbmask = (unsigned)(P.g.nb - 1);
+
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(P.work, 1ull);
+        item = __shfl_sync(full, item, 0);
+        if ((int64_t)item >= n_items) break;
+        const int t = (int)((int64_t)item / nA);
+        const int a = P.a_order[(int64_t)item % nA];
+        const int64_t a0 = P.A.off[a];
+        const int na = (int)(P.A.off[a + 1] - a0);
+        const int b_begin = t * P.g.tile;
+        const int tn = (int)min((int64_t)P.g.tile, P.B.n - b_begin);
+        const int64_t tbase = P.B.off[b_begin];
+        const uint32_t* T = P.tab + (int64_t)t * (P.g.nb + 1);
+        const double snA = P.snA[a];
+
+        int width = tn;
+        if (P.init_width_scale > 0.f && na > 0)
+            width = max(32, min(tn, (int)(P.init_width_scale / (float)na)));
+        int range_lo = 0;
+        while (range_lo < tn) {
+            const int range_hi = min(range_lo + width, tn);
+            const int rw = range_hi - range_lo;
+            // ---- sweep: collect candidates of (a, queries [range_lo, range_hi)) ----
+            for (int w = lane; w < (rw + 31) / 32; w += 32) W.hasbits[w] = 0u;
+            if (lane == 0) W.n = 0;
+            __syncwarp();
+            for (int pc = 0; pc < na; pc += 32) {
+                const int p = pc + lane;
+                if (p < na) {
+                    const double mzA = (double)P.A.mz[a0 + p];
+                    double lo_a = 0.0, hi_a = 0.0, mz2_a = 0.0, slo, shi;
+                    if (A_IS_REF) {
+                        lo_a = __dsub_rn(mzA, P.tol);
+                        hi_a = __dadd_rn(mzA, P.tol);
+                        slo = __dsub_rn(lo_a, P.shift);
+                        shi = __dsub_rn(hi_a, P.shift);
+                    } else {
+                        mz2_a = __dadd_rn(mzA, P.shift);
+                        slo = __dsub_rn(mz2_a, P.tol);
+                        shi = __dadd_rn(mz2_a, P.tol);
+                    }
+                    long long blo = bucket_of(slo, P.g.inv_w) - P.widen;
+                    long long bhi = bucket_of(shi, P.g.inv_w) + P.widen;
+                    if (bhi - blo + 1 >= P.g.nb) {
+                        blo = 0;
+                        bhi = P.g.nb - 1;
+                    }
+                    double wA = -1.0;  // a*b of this A peak, loaded on first candidate
+                    for (long long b = blo; b <= bhi; ++b) {
+                        const unsigned bk = (unsigned)b & nbmask;
+                        const uint32_t e0 = T[bk], e1 = T[bk + 1];
+                        for (uint32_t e = e0; e < e1; ++e) {
+                            const uint2 en = P.ent[tbase + e];
+                            const int bq = (int)(en.y >> 16);
+                            if (bq < range_lo || bq >= range_hi) continue;
+                            const double mzB = (double)__uint_as_float(en.x);
+                            bool match;
+                            if (A_IS_REF) {
+                                const double mz2 = __dadd_rn(mzB, P.shift);
+                                match = !(mz2 > hi_a) && !(mz2 < lo_a);
+                            } else {
+                                const double lo_b = __dsub_rn(mzB, P.tol);
+                                const double hi_b = __dadd_rn(mzB, P.tol);
+                                match = !(mz2_a > hi_b) && !(mz2_a < lo_b);
+                            }
+                            if (!match) continue;
+                            const int pB = (int)(en.y & 0xFFFFu);
+                            const int64_t gB = P.B.off[b_begin + bq] + pB;
+                            if (wA < 0.0) wA = __dmul_rn(peak_a(P.A.a, a0 + p), P.A.b[a0 + p]);
+                            double key;
+                            uint32_t gen;
+                            if (A_IS_REF) {
+                                key = __dmul_rn(__dmul_rn(wA, peak_a(P.B.a, gB)), P.B.b[gB]);
+                                gen = ((uint32_t)p << 16) | (uint32_t)pB;
+                            } else {
+                                const double wB = __dmul_rn(peak_a(P.B.a, gB), P.B.b[gB]);
+                                key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + p)),
+                                                P.A.b[a0 + p]);
+                                gen = ((uint32_t)pB << 16) | (uint32_t)p;
+                            }
+                            const int slot = atomicAdd(&W.n, 1);
+                            if (slot < kPool) {
+                                const int qr = bq - range_lo;
+                                W.key[slot] = key;
+                                W.gen[slot] = gen;
+                                W.sk[slot] = ((uint32_t)qr << 16) | (uint32_t)slot;
+                                atomicOr(&W.hasbits[qr >> 5], 1u << (qr & 31));
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                const int n_now = *(volatile int*)&W.n;
+                __syncwarp();
+                if (n_now > kPool) break;
+            }
+            __syncwarp();
+            const int n = *(volatile int*)&W.n;
+            if (n > kPool) {
+                if (rw > 1) {
+                    // too many candidates for one pool: retry a narrower range
+                    width = max(1, (int)((long long)rw * kPool / (2LL * n)));
+                    width = min(width, rw / 2 > 0 ? rw / 2 : 1);
+                    __syncwarp();
+                    continue;
+                }
+                // a single pair has more candidates than the pool: pair kernel
+                if (lane == 0) {
+                    const int bq = b_begin + range_lo;
+                    const int rr = A_IS_REF ? a : bq, qq = A_IS_REF ? bq : a;
+                    spill_push(P.spill, rr, qq, P.err);
+                    if (!SPARSE) {
+                        const int64_t o = (int64_t)rr * P.dense.ld + qq;
+                        P.dense.score[o] = __int_as_float(0x7fc00000);
+                        P.dense.matches[o] = -1;
+                        P.dense.overflow[o] = 0;
+                    }
+                }
+                __syncwarp();
+                range_lo = range_hi;
+                width = max(32, width);
+                continue;
+            }
+
+            // ---- group the pool by query: sort (q_rel, slot) ----
+            if (n > 1) {
+                int m = 2;
+                while (m < n) m <<= 1;
+                for (int i = n + lane; i < m; i += 32) W.sk[i] = 0xffffffffu;
+                __syncwarp();
+                warp_bitonic_u32(W.sk, m, lane);
+            }
+            // run starts
+            int n_runs = 0;
+            for (int c = 0; c < n; c += 32) {
+                const int i = c + lane;
+                bool start = false;
+                if (i < n) start = (i == 0) || ((W.sk[i] >> 16) != (W.sk[i - 1] >> 16));
+                const unsigned bal = __ballot_sync(full, start);
+                if (start) W.run_start[n_runs + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
+                n_runs += __popc(bal);
+            }
+            if (lane == 0) W.run_start[n_runs] = (uint16_t)n;
+            __syncwarp();
+
+            // ---- resolve each run (one lane per query) ----
+            for (int r = lane; r < n_runs; r += 32) {
+                const int s = W.run_start[r], e = W.run_start[r + 1];
+                const int L = e - s;
+                const int qr = (int)(W.sk[s] >> 16);
+                const int bq = b_begin + range_lo + qr;
+                const int rr = A_IS_REF ? a : bq, qq = A_IS_REF ? bq : a;
+                float sc;
+                int mt;
+                if (L >= P.match_limit || L > kSmallRun) {
+                    spill_push(P.spill, rr, qq, P.err);
+                    sc = __int_as_float(0x7fc00000);
+                    mt = -1;
+                } else {
+                    double score = 0.0;
+                    int matches = 0;
+                    if (L == 1) {
+                        score = W.key[W.sk[s] & 0xFFFFu];
+                        matches = 1;
+                    } else {
+                        // selection in greedy order; conflicts against accepted
+                        unsigned done = 0, acc = 0;
+                        for (int it = 0; it < L; ++it) {
+                            int best = -1;
+                            double bk = 0.0;
+                            uint32_t bg = 0;
+                            for (int x = 0; x < L; ++x) {
+                                if (done & (1u << x)) continue;
+                                const int sl = (int)(W.sk[s + x] & 0xFFFFu);
+                                const double k = W.key[sl];
+                                const uint32_t gg = W.gen[sl];
+                                if (best < 0 || before(k, gg, bk, bg)) {
+                                    best = x;
+                                    bk = k;
+                                    bg = gg;
+                                }
+                            }
+                            done |= 1u << best;
+                            bool ok = true;
+                            for (unsigned m2 = acc; m2; m2 &= m2 - 1) {
+                                const int x = __ffs(m2) - 1;
+                                const uint32_t gx = W.gen[W.sk[s + x] & 0xFFFFu];
+                                if ((gx >> 16) == (bg >> 16) || (gx & 0xFFFFu) == (bg & 0xFFFFu)) {
+                                    ok = false;
+                                    break;
+                                }
+                            }
+                            if (ok) {
+                                acc |= 1u << best;
+                                score = __dadd_rn(score, bk);
+                                ++matches;
+                            }
+                        }
+                    }
+                    const double snB = P.snB[bq];
+                    const double denom = A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA);
+                    sc = (float)__ddiv_rn(score, denom);
+                    mt = matches;
+                }
+                W.res_score[r] = sc;
+                W.res_matches[r] = mt;
+            }
+            __syncwarp();
+
+            // ---- write results ----
+            if (!SPARSE) {
+                // dense row segment out[a, b_begin + range_lo ...), coalesced
+                int rank_base = 0;
+                const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
+                for (int c = 0; c < rw; c += 32) {
+                    const int qr = c + lane;
+                    const uint32_t word = W.hasbits[c >> 5];
+                    if (qr < rw) {
+                        float sc = 0.f;
+                        int mt = 0;
+                        if ((word >> lane) & 1u) {
+                            const int rk = rank_base + __popc(word & ((1u << lane) - 1u));
+                            sc = W.res_score[rk];
+                            mt = W.res_matches[rk];
+                        }
+                        // a spilled pair gets (NaN, -1, 0) here; the pair kernel,
+                        // launched after this one on the same stream, overwrites it
+                        P.dense.score[row + qr] = sc;
+                        P.dense.matches[row + qr] = mt;
+                        P.dense.overflow[row + qr] = 0;
+                    }
+                    rank_base += __popc(word);
+                }
+            } else {
+                for (int c = 0; c < n_runs; c += 32) {
+                    const int r = c + lane;
+                    bool hit = false;
+                    float sc = 0.f;
+                    int mt = 0, bq = 0;
+                    if (r < n_runs) {
+                        sc = W.res_score[r];
+                        mt = W.res_matches[r];
+                        bq = b_begin + range_lo + (int)(W.sk[W.run_start[r]] >> 16);
+                        hit = mt >= 0 && sc >= P.sparse.threshold;
+                    }
+                    const unsigned bal = __ballot_sync(full, hit);
+                    if (bal) {
+                        unsigned long long base = 0;
+                        if (lane == 0) base = atomicAdd(P.sparse.count, (unsigned long long)__popc(bal));
+                        base = __shfl_sync(full, base, 0);
+                        if (hit) {
+                            const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
+                            if (pos < (unsigned long long)P.sparse.capacity) {
+                                P.sparse.r[pos] = A_IS_REF ? a : bq;
+                                P.sparse.q[pos] = A_IS_REF ? bq : a;
+                                P.sparse.score[pos] = sc;
+                                P.sparse.matches[pos] = mt;
+                                P.sparse.overflow[pos] = 0;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            range_lo = range_hi;
+            if (n < kPool / 4) width = min(tn, width * 2);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 6. pair kernel: one CTA per pair
+// ---------------------------------------------------------------------------
+struct PairParams {
+    SpecSet R;
+    SpecSet Q;
+    const double* snR;
+    const double* snQ;
+    double tol;
+    double shift;
+    int match_limit;
+    int cap;  // power of two >= match_limit
+    // work: either the spill list (pairs != nullptr) or every pair of R x Q
+    const int2* pairs;
+    const unsigned int* n_pairs;
+    unsigned int pairs_cap;
+    unsigned long long* work;
+    DenseOut dense;
+    SparseOut sparse;
+    uint32_t* err;
+    const uint32_t* bad;
+};
+
+template <bool SPARSE>
+__global__ void pair_kernel(PairParams P) {
+    if (*P.bad) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned long long* okey = reinterpret_cast<unsigned long long*>(smem_raw);
+    uint32_t* cgen = reinterpret_cast<uint32_t*>(okey + P.cap);
+    uint32_t* used_r = cgen + P.cap;          // 2048 words: 65536 peaks
+    uint32_t* used_q = used_r + 2048;
+    __shared__ int s_scan[32];
+    __shared__ unsigned long long s_item;
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const unsigned full = 0xffffffffu;
+    const int64_t n_items = P.pairs ? (int64_t)min(*P.n_pairs, P.pairs_cap) : P.R.n * P.Q.n;
+
+    for (int64_t iter = 0;; ++iter) {
+        // spill list: dynamic (pairs differ widely in cost); whole matrix:
+        // static stride (uniform pairs, no contention on one counter)
+        __syncthreads();
+        if (tid == 0) s_item = P.pairs ? atomicAdd(P.work, 1ull)
+                                       : (unsigned long long)(blockIdx.x + iter * gridDim.x);
+        __syncthreads();
+        const int64_t item = (int64_t)s_item;
+        if (item >= n_items) break;
+        int64_t ri, qi;
+        if (P.pairs) {
+            const int2 pr = P.pairs[item];
+            ri = pr.x;
+            qi = pr.y;
+        } else {
+            ri = item / P.Q.n;
+            qi = item - ri * P.Q.n;
+        }
+        const int64_t r0 = P.R.off[ri], q0 = P.Q.off[qi];
+        const int nr = (int)(P.R.off[ri + 1] - r0), nq = (int)(P.Q.off[qi + 1] - q0);
+        const float* qmz = P.Q.mz + q0;
+
+        int total = 0;
+        bool overflow = false;
+        if (nr > 0 && nq > 0) {
+            for (int pc = 0; pc < nr && !overflow; pc += blockDim.x) {
+                const int p1 = pc + tid;
+                int start = 0, cnt = 0;
+                double lo = 0.0, hi = 0.0, w1 = 0.0;
+                if (p1 < nr) {
+                    const double mz1 = (double)P.R.mz[r0 + p1];
+                    lo = __dsub_rn(mz1, P.tol);
+                    hi = __dadd_rn(mz1, P.tol);
+                    // first p2 with mz_q + shift >= lo
+                    int L = 0, H = nq;
+                    while (L < H) {
+                        const int M = (L + H) >> 1;
+                        if (__dadd_rn((double)qmz[M], P.shift) < lo)
+                            L = M + 1;
+                        else
+                            H = M;
+                    }
+                    start = L;
+                    int k = L;
+                    while (k < nq && !(__dadd_rn((double)qmz[k], P.shift) > hi)) ++k;
+                    cnt = k - L;
+                }
+                // block exclusive scan of cnt
+                int incl = cnt;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(full, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                if (lane == 31) s_scan[wid] = incl;
+                __syncthreads();
+                if (wid == 0) {
+                    int v = lane < nwarps ? s_scan[lane] : 0;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const int u = __shfl_up_sync(full, v, d);
+                        if (lane >= d) v += u;
+                    }
+                    if (lane < nwarps) s_scan[lane] = v;
+                }
+                __syncthreads();
+                const int excl = incl - cnt + (wid > 0 ? s_scan[wid - 1] : 0);
+                const int chunk_total = s_scan[nwarps - 1];
+                if (cnt > 0) {
+                    w1 = __dmul_rn(peak_a(P.R.a, r0 + p1), P.R.b[r0 + p1]);
+                    for (int i = 0; i < cnt; ++i) {
+                        const int rank = total + excl + i;
+                        if (rank >= P.match_limit) break;
+                        const int p2 = start + i;
+                        const double key =
+                            __dmul_rn(__dmul_rn(w1, peak_a(P.Q.a, q0 + p2)), P.Q.b[q0 + p2]);
+                        okey[rank] = order_key(key);
+                        cgen[rank] = ((uint32_t)p1 << 16) | (uint32_t)p2;
+                    }
+                }
+                total += chunk_total;
+                if (total >= P.match_limit) overflow = true;
+                __syncthreads();
+            }
+        }
+        const int n = min(total, P.match_limit);
+        double score = 0.0;
+        int matches = 0;
+        if (n > 0) {
+            int m = 1;
+            while (m < n) m <<= 1;
+            for (int i = n + tid; i < m; i += blockDim.x) {
+                okey[i] = 0ull;
+                cgen[i] = 0u;
+            }
+            for (int i = tid; i < (nr + 31) / 32; i += blockDim.x) used_r[i] = 0u;
+            for (int i = tid; i < (nq + 31) / 32; i += blockDim.x) used_q[i] = 0u;
+            __syncthreads();
+            // bitonic sort, descending by (okey, gen)
+            for (int k = 2; k <= m; k <<= 1) {
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = tid; i < m; i += blockDim.x) {
+                        const int ixj = i ^ j;
+                        if (ixj > i) {
+                            const unsigned long long ka = okey[i], kb = okey[ixj];
+                            const uint32_t ga = cgen[i], gb = cgen[ixj];
+                            const bool a_gt_b = ka > kb || (ka == kb && ga > gb);
+                            const bool desc = (i & k) == 0;
+                            if (desc ? !a_gt_b : a_gt_b) {
+                                okey[i] = kb;
+                                okey[ixj] = ka;
+                                cgen[i] = gb;
+                                cgen[ixj] = ga;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            // greedy by warp 0: chunks of 32 in order, leaders in lane order
+            if (wid == 0) {
+                for (int c = 0; c < n; c += 32) {
+                    const int i = c + lane;
+                    uint32_t g = 0;
+                    double kk = 0.0;
+                    bool alive = false;
+                    if (i < n) {
+                        g = cgen[i];
+                        kk = key_from_order(okey[i]);
+                        const int p1 = g >> 16, p2 = g & 0xFFFF;
+                        alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
+                                !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
+                    }
+                    unsigned bal = __ballot_sync(full, alive);
+                    while (bal) {
+                        const int leader = __ffs(bal) - 1;
+                        const uint32_t lg = __shfl_sync(full, g, leader);
+                        const double lk = __shfl_sync(full, kk, leader);
+                        if (lane == 0) {
+                            score = __dadd_rn(score, lk);
+                            ++matches;
+                        }
+                        if (lane == leader) {
+                            const int p1 = lg >> 16, p2 = lg & 0xFFFF;
+                            used_r[p1 >> 5] |= 1u << (p1 & 31);
+                            used_q[p2 >> 5] |= 1u << (p2 & 31);
+                            alive = false;
+                        }
+                        if (alive && (((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu))))
+                            alive = false;
+                        bal = __ballot_sync(full, alive);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        if (tid == 0) {
+            float sc = 0.f;
+            if (matches > 0 || n > 0) {
+                const double denom = __dmul_rn(P.snR[ri], P.snQ[qi]);
+                sc = (n > 0) ? (float)__ddiv_rn(score, denom) : 0.f;
+            }
+            if (!SPARSE) {
+                const int64_t o = ri * P.dense.ld + qi;
+                P.dense.score[o] = sc;
+                P.dense.matches[o] = matches;
+                P.dense.overflow[o] = overflow ? 1 : 0;
+            } else if (n > 0 && sc >= P.sparse.threshold) {
+                const unsigned long long pos = atomicAdd(P.sparse.count, 1ull);
+                if (pos < (unsigned long long)P.sparse.capacity) {
+                    P.sparse.r[pos] = (int32_t)ri;
+                    P.sparse.q[pos] = (int32_t)qi;
+                    P.sparse.score[pos] = sc;
+                    P.sparse.matches[pos] = matches;
+                    P.sparse.overflow[pos] = overflow ? 1 : 0;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+inline int next_pow2(long long x) {
+    int p = 1;
+    while (p < x && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+struct Plan {
+    int mode;
+    int tile;
+    int n_tiles;
+    int nb;
+    double width;
+    int pair_threads;
+    int cap;
+    unsigned int spill_cap;
+};
+
+int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse, Plan& p) {
+    p.mode = (cfg && cfg->mode) ? cfg->mode : 1;
+    if (p.mode != 1 && p.mode != 2) {
+        set_error("cms_cosine_greedy: mode must be 0, 1 or 2");
+        return CMS_ERR_INVALID;
+    }
+    p.tile = (cfg && cfg->tile_spectra > 0) ? cfg->tile_spectra : 1024;
+    if (p.tile > kMaxTile) {
+        set_error("cms_cosine_greedy: tile_spectra must be <= %d", kMaxTile);
+        return CMS_ERR_UNSUPPORTED;
+    }
+    p.tile = (int)std::min<int64_t>(p.tile, std::max<int64_t>(1, args.qry.n));
+    p.n_tiles = (int)((args.qry.n + p.tile - 1) / p.tile);
+    double w = (cfg && cfg->bucket_width > 0.0) ? cfg->bucket_width : 2.0 * args.tol;
+    if (w < args.tol) w = args.tol;
+    if (!(w > 0.0)) w = 1e-3;
+    p.width = w;
+    const double avg_tile_peaks =
+        args.qry.n > 0 ? (double)args.qry.n_peaks * p.tile / (double)args.qry.n : 1.0;
+    p.nb = (cfg && cfg->n_buckets > 0) ? next_pow2(cfg->n_buckets)
+                                       : next_pow2((long long)std::max(1024.0, avg_tile_peaks));
+    p.nb = std::min(p.nb, 1 << 22);
+    p.pair_threads = (cfg && cfg->pair_threads > 0) ? cfg->pair_threads : 128;
+    if (p.pair_threads < 64 || p.pair_threads > 512 || p.pair_threads % 32) {
+        set_error("cms_cosine_greedy: pair_threads must be a multiple of 32 in [64, 512]");
+        return CMS_ERR_INVALID;
+    }
+    p.cap = next_pow2(std::max(2, args.match_limit));
+    const long long pairs = (long long)args.ref.n * (long long)args.qry.n;
+    long long sc = std::max<long long>(1 << 20, pairs / 64);
+    sc = std::min<long long>(sc, std::min<long long>(pairs, 1LL << 28));
+    p.spill_cap = (unsigned int)std::max<long long>(sc, 1);
+    (void)sparse;
+    return CMS_OK;
+}
+
+template <typename T>
+void set_func_smem(T* f, size_t bytes) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
+               const SparseOut* sparse, const cms_cosine_config* cfg, cudaStream_t s) {
+    Plan p;
+    int rc = make_plan(args, cfg, sparse != nullptr, p);
+    if (rc) return rc;
+    const size_t pair_smem = (size_t)p.cap * 12 + 2 * 2048 * 4;
+    if (pair_smem > ctx->smem_optin) {
+        set_error("cms_cosine_greedy: match_limit %d needs %zu B shared memory (> %zu)",
+                  args.match_limit, pair_smem, ctx->smem_optin);
+        return CMS_ERR_UNSUPPORTED;
+    }
+
+    // ---- scratch layout ----
+    const int64_t nR = args.ref.n, nQ = args.qry.n;
+    size_t need = 0;
+    need += bump_size(64 * sizeof(uint64_t));            // flags, counters
+    need += bump_size(nR * sizeof(double)) + bump_size(nQ * sizeof(double));
+    if (p.mode == 1) {
+        need += bump_size(nR * sizeof(int32_t));
+        need += bump_size((size_t)p.n_tiles * (p.nb + 1) * sizeof(uint32_t));
+        need += bump_size((size_t)p.n_tiles * p.nb * sizeof(uint32_t));
+        need += bump_size((size_t)std::max<int64_t>(1, args.qry.n_peaks) * sizeof(uint2));
+        need += bump_size((size_t)p.spill_cap * sizeof(int2));
+    }
+    need += 4096;
+    rc = arena_reserve(ctx, ctx->scratch, need, s);
+    if (rc) return rc;
+    Bump bp{(char*)ctx->scratch.ptr, 0, ctx->scratch.bytes};
+    uint64_t* small = bp.take<uint64_t>(64);
+    uint32_t* bad = reinterpret_cast<uint32_t*>(small);            // word 0
+    uint32_t* cls_count = reinterpret_cast<uint32_t*>(small + 1);  // 17 words
+    uint32_t* cls_cursor = reinterpret_cast<uint32_t*>(small + 10);  // 17 words
+    unsigned int* spill_count = reinterpret_cast<unsigned int*>(small + 20);
+    unsigned long long* work_join = reinterpret_cast<unsigned long long*>(small + 21);
+    unsigned long long* work_pair = reinterpret_cast<unsigned long long*>(small + 22);
+    double* snR = bp.take<double>(nR);
+    double* snQ = bp.take<double>(nQ);
+    CMS_CUDA_TRY(cudaMemsetAsync(small, 0, 64 * sizeof(uint64_t), s));
+
+    const int threads = 256;
+    auto grid_for = [&](int64_t n, int per_block) {
+        int64_t g = (n + per_block - 1) / per_block;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)ctx->sm_count * 32));
+    };
+    {
+        StageScope sc(ctx, 0, 4, s);
+        validate_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, bad, ctx->err_word);
+        validate_kernel<<<grid_for(nQ, threads), threads, 0, s>>>(args.qry, bad, ctx->err_word);
+        norms_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, snR, bad);
+        norms_kernel<<<grid_for(nQ, threads), threads, 0, s>>>(args.qry, snQ, bad);
+    }
+    CMS_CUDA_TRY(cudaGetLastError());
+
+    if (sparse) CMS_CUDA_TRY(cudaMemsetAsync(sparse->count, 0, sizeof(unsigned long long), s));
+
+    PairParams pp;
+    pp.R = args.ref;
+    pp.Q = args.qry;
+    pp.snR = snR;
+    pp.snQ = snQ;
+    pp.tol = args.tol;
+    pp.shift = args.shift;
+    pp.match_limit = args.match_limit;
+    pp.cap = p.cap;
+    pp.pairs = nullptr;
+    pp.n_pairs = nullptr;
+    pp.pairs_cap = 0;
+    pp.work = work_pair;
+    pp.dense = dense ? *dense : DenseOut{nullptr, nullptr, nullptr, 0};
+    pp.sparse = sparse ? *sparse : SparseOut{};
+    pp.err = ctx->err_word;
+    pp.bad = bad;
+
+    int pair_blocks_per_sm = 1;
+    if (sparse) {
+        set_func_smem(pair_kernel<true>, pair_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<true>,
+                                                      p.pair_threads, pair_smem);
+    } else {
+        set_func_smem(pair_kernel<false>, pair_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<false>,
+                                                      p.pair_threads, pair_smem);
+    }
+    pair_blocks_per_sm = std::max(1, pair_blocks_per_sm);
+    const int pair_grid = ctx->sm_count * pair_blocks_per_sm;
+
+    if (p.mode == 2) {
+        StageScope sc(ctx, 4, 1, s);
+        if (sparse)
+            pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        else
+            pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        CMS_CUDA_TRY(cudaGetLastError());
+        return CMS_OK;
+    }
+
+    // ---- mode 1: order, index, join, spill ----
+    int32_t* order = bp.take<int32_t>(nR);
+    uint32_t* tab = bp.take<uint32_t>((size_t)p.n_tiles * (p.nb + 1));
+    uint32_t* cur = bp.take<uint32_t>((size_t)p.n_tiles * p.nb);
+    uint2* ent = bp.take<uint2>((size_t)std::max<int64_t>(1, args.qry.n_peaks));
+    int2* spill = bp.take<int2>(p.spill_cap);
+
+    {
+        StageScope sc(ctx, 1, 2, s);
+        order_count_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, cls_count, bad);
+        order_scatter_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, cls_count,
+                                                                       cls_cursor, order, bad);
+    }
+    IndexGeom g{p.tile, p.n_tiles, p.nb, 1.0 / p.width};
+    {
+        StageScope sc(ctx, 2, 3, s);
+        CMS_CUDA_TRY(cudaMemsetAsync(cur, 0, (size_t)p.n_tiles * p.nb * sizeof(uint32_t), s));
+        index_count_kernel<<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur, bad);
+        index_scan_kernel<<<p.n_tiles, 1024, 0, s>>>(g, cur, tab, bad);
+        index_scatter_kernel<<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur,
+                                                                            ent, bad);
+    }
+    CMS_CUDA_TRY(cudaGetLastError());
+
+    JoinParams jp;
+    jp.A = args.ref;
+    jp.B = args.qry;
+    jp.snA = snR;
+    jp.snB = snQ;
+    jp.a_order = order;
+    jp.tab = tab;
+    jp.ent = ent;
+    jp.g = g;
+    jp.tol = args.tol;
+    jp.shift = args.shift;
+    jp.match_limit = args.match_limit;
+    jp.widen = args.shift != 0.0 ? 1 : 0;
+    jp.init_width_scale = 0.f;
+    jp.work = work_join;
+    jp.spill = SpillList{spill, spill_count, p.spill_cap};
+    jp.dense = pp.dense;
+    jp.sparse = pp.sparse;
+    jp.err = ctx->err_word;
+    jp.bad = bad;
+    const size_t join_smem = sizeof(WarpSmem) * kJoinWarps;
+    int join_blocks_per_sm = 1;
+    {
+    StageScope sc(ctx, 3, 1, s);
+    if (sparse) {
+        set_func_smem(join_kernel<true, true>, join_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, true>,
+                                                      kJoinThreads, join_smem);
+        join_kernel<true, true><<<ctx->sm_count * std::max(1, join_blocks_per_sm), kJoinThreads,
+                                  join_smem, s>>>(jp);
+    } else {
+        set_func_smem(join_kernel<true, false>, join_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, false>,
+                                                      kJoinThreads, join_smem);
+        join_kernel<true, false><<<ctx->sm_count * std::max(1, join_blocks_per_sm), kJoinThreads,
+                                   join_smem, s>>>(jp);
+    }
+    }
+    CMS_CUDA_TRY(cudaGetLastError());
+
+    pp.pairs = spill;
+    pp.n_pairs = spill_count;
+    pp.pairs_cap = p.spill_cap;
+    StageScope sc(ctx, 4, 1, s);
+    if (sparse)
+        pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+    else
+        pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+    CMS_CUDA_TRY(cudaGetLastError());
+    return CMS_OK;
+}
+
+bool check_common(const CosineArgs& a, const char* who) {
+    if (!check_specset(a.ref, "reference") || !check_specset(a.qry, "query")) return false;
+    if (a.match_limit < 1 || !(a.tol >= 0.0) || !std::isfinite(a.tol) || !std::isfinite(a.shift)) {
+        set_error("%s: invalid match_limit or tolerance/shift", who);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace cms
+
+extern "C" int cms_cosine_greedy(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                                 const double* ref_b, const int64_t* ref_off, int64_t n_ref,
+                                 int64_t n_ref_peaks, const float* q_mz, const double* q_a,
+                                 const double* q_b, const int64_t* q_off, int64_t n_q,
+                                 int64_t n_q_peaks, double tolerance, double shift,
+                                 int match_limit, float* score, int32_t* matches,
+                                 uint8_t* overflow, int64_t ld, const cms_cosine_config* cfg,
+                                 void* stream) {
+    using namespace cms;
+    if (!ctx) {
+        set_error("cms_cosine_greedy: null context");
+        return CMS_ERR_INVALID;
+    }
+    CosineArgs args{SpecSet{ref_mz, ref_a, ref_b, ref_off, n_ref, n_ref_peaks},
+                    SpecSet{q_mz, q_a, q_b, q_off, n_q, n_q_peaks}, tolerance, shift,
+                    match_limit};
+    if (!check_common(args, "cms_cosine_greedy")) return CMS_ERR_INVALID;
+    if (ld < n_q) {
+        set_error("cms_cosine_greedy: ld < n_q");
+        return CMS_ERR_INVALID;
+    }
+    if (n_ref == 0 || n_q == 0) return CMS_OK;
+    if (!score || !matches || !overflow) {
+        set_error("cms_cosine_greedy: null output pointer");
+        return CMS_ERR_INVALID;
+    }
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    DenseOut out{score, matches, overflow, ld};
+    return run_cosine(ctx, args, &out, nullptr, cfg, (cudaStream_t)stream);
+}
+
+extern "C" int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                                        const double* ref_b, const int64_t* ref_off, int64_t n_ref,
+                                        int64_t n_ref_peaks, const float* q_mz,
+                                        const double* q_a, const double* q_b,
+                                        const int64_t* q_off, int64_t n_q, int64_t n_q_peaks,
+                                        double tolerance, double shift, int match_limit,
+                                        float threshold, int32_t* hit_ref, int32_t* hit_query,
+                                        float* hit_score, int32_t* hit_matches,
+                                        uint8_t* hit_overflow, int64_t capacity,
+                                        int64_t* hit_count, const cms_cosine_config* cfg,
+                                        void* stream) {
+    using namespace cms;
+    if (!ctx) {
+        set_error("cms_cosine_greedy_sparse: null context");
+        return CMS_ERR_INVALID;
+    }
+    CosineArgs args{SpecSet{ref_mz, ref_a, ref_b, ref_off, n_ref, n_ref_peaks},
+                    SpecSet{q_mz, q_a, q_b, q_off, n_q, n_q_peaks}, tolerance, shift,
+                    match_limit};
+    if (!check_common(args, "cms_cosine_greedy_sparse")) return CMS_ERR_INVALID;
+    if (!(threshold > 0.0f)) {
+        set_error("cms_cosine_greedy_sparse: threshold must be > 0 (every pair scores >= 0)");
+        return CMS_ERR_INVALID;
+    }
+    if (capacity < 0 || !hit_count || (capacity > 0 && (!hit_ref || !hit_query || !hit_score ||
+                                                        !hit_matches || !hit_overflow))) {
+        set_error("cms_cosine_greedy_sparse: invalid hit buffers");
+        return CMS_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (n_ref == 0 || n_q == 0) {
+        CMS_CUDA_TRY(cudaMemsetAsync(hit_count, 0, sizeof(int64_t), s));
+        return CMS_OK;
+    }
+    SparseOut out{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
+                  reinterpret_cast<unsigned long long*>(hit_count), threshold};
+    return run_cosine(ctx, args, nullptr, &out, cfg, s);
+}

@@ -1,0 +1,185 @@
+"""Device calls: torch tensors as buffers, libcudams_b200.so for the compute.
+
+These functions are the only place that hands device pointers to the C ABI.
+They enqueue work on the current (or given) torch CUDA stream and return
+device tensors; `check=True` synchronises the stream and raises if a kernel
+reported bad input through the context's error word.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import torch
+
+from . import _native
+from ._native import CosineConfig, NativeError, check, ptr, stream_handle
+from .packing import DeviceSpectra
+
+
+def _cfg(config: Optional[dict]):
+    if not config:
+        return None
+    c = CosineConfig()
+    for k, v in config.items():
+        setattr(c, k, v)
+    return c
+
+
+def _stream(device, stream):
+    return stream if stream is not None else torch.cuda.current_stream(device)
+
+
+def _raise_device_error(bits: int, what: str) -> None:
+    if not bits:
+        return
+    parts = []
+    if bits & _native.DEVERR_SPECTRUM_TOO_LONG:
+        parts.append("a spectrum has more than 65535 peaks")
+    if bits & _native.DEVERR_BAD_OFFSETS:
+        parts.append("spectrum offsets are not non-decreasing within the peak arrays")
+    if bits & _native.DEVERR_SPILL_OVERRUN:
+        parts.append("spill list overrun")
+    raise NativeError(f"{what}: device reported bad input ({'; '.join(parts)})",
+                      _native.CMS_ERR_DEVICE)
+
+
+def take_device_error(device, stream=None) -> int:
+    s = _stream(device, stream)
+    return _native.context(device.index).take_device_error(stream_handle(s))
+
+
+def cosine_greedy_dense(ref: DeviceSpectra, qry: DeviceSpectra, tolerance: float, shift: float,
+                        match_limit: int, *, out=None, config: Optional[dict] = None,
+                        stream=None, check_errors: bool = False):
+    """Greedy cosine for all pairs -> (score f32, matches i32, overflow u8) [n_ref, n_q]."""
+    lib = _native.load()
+    device = ref.mz.device if ref.mz is not None else qry.mz.device
+    s = _stream(device, stream)
+    if out is None:
+        out = (torch.empty((ref.n, qry.n), dtype=torch.float32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.int32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.uint8, device=device))
+    score, matches, overflow = out
+    ld = score.stride(0) if score.dim() == 2 else qry.n
+    ctx = _native.context(device.index)
+    cfg = _cfg(config)
+    rc = lib.cms_cosine_greedy(
+        ctx.handle, ptr(ref.mz), ptr(ref.a), ptr(ref.b), ptr(ref.offsets), ref.n, ref.n_peaks,
+        ptr(qry.mz), ptr(qry.a), ptr(qry.b), ptr(qry.offsets), qry.n, qry.n_peaks,
+        float(tolerance), float(shift), int(match_limit), ptr(score), ptr(matches),
+        ptr(overflow), int(ld), None if cfg is None else _ctypes_ref(cfg), stream_handle(s))
+    check(rc, "cms_cosine_greedy")
+    if check_errors:
+        bits = ctx.take_device_error(stream_handle(s))
+        if bits & _native.DEVERR_SPILL_OVERRUN and not (config or {}).get("mode") == 2:
+            # rare: too many long-candidate pairs for the spill list; redo with
+            # the pair kernel over the whole matrix
+            cfg2 = dict(config or {})
+            cfg2["mode"] = 2
+            return cosine_greedy_dense(ref, qry, tolerance, shift, match_limit, out=out,
+                                       config=cfg2, stream=stream, check_errors=True)
+        _raise_device_error(bits, "cms_cosine_greedy")
+    return score, matches, overflow
+
+
+def _ctypes_ref(obj):
+    import ctypes
+
+    return ctypes.byref(obj)
+
+
+def cosine_greedy_plain(ref: DeviceSpectra, qry: DeviceSpectra, tolerance: float, shift: float,
+                        match_limit: int, n_max_peaks: int, *, out=None, stream=None):
+    """The plain one-pair-per-thread kernel (benchmark comparator)."""
+    lib = _native.load()
+    device = ref.mz.device
+    s = _stream(device, stream)
+    if out is None:
+        out = (torch.empty((ref.n, qry.n), dtype=torch.float32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.int32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.uint8, device=device))
+    score, matches, overflow = out
+    ld = score.stride(0)
+    rc = lib.cms_cosine_greedy_plain(
+        ptr(ref.mz), ptr(ref.a), ptr(ref.b), ptr(ref.offsets), ref.n,
+        ptr(qry.mz), ptr(qry.a), ptr(qry.b), ptr(qry.offsets), qry.n,
+        float(tolerance), float(shift), int(match_limit), int(n_max_peaks),
+        ptr(score), ptr(matches), ptr(overflow), int(ld), stream_handle(s))
+    check(rc, "cms_cosine_greedy_plain")
+    return score, matches, overflow
+
+
+class SparseHits:
+    """Device hit arrays of one sparse call (the first `count` entries are valid)."""
+
+    def __init__(self, r, q, score, matches, overflow, count):
+        self.r, self.q, self.score, self.matches, self.overflow = r, q, score, matches, overflow
+        self.count = count
+
+    def to_host(self, sort: bool = True):
+        import numpy as np
+
+        n = int(self.count)
+        r = self.r[:n].cpu().numpy()
+        q = self.q[:n].cpu().numpy()
+        sc = self.score[:n].cpu().numpy()
+        mt = self.matches[:n].cpu().numpy()
+        ov = self.overflow[:n].cpu().numpy()
+        if sort and n:
+            o = np.lexsort((q, r))
+            r, q, sc, mt, ov = r[o], q[o], sc[o], mt[o], ov[o]
+        return r, q, sc, mt, ov
+
+
+def cosine_greedy_sparse(ref: DeviceSpectra, qry: DeviceSpectra, tolerance: float, shift: float,
+                         match_limit: int, threshold: float, *, capacity: Optional[int] = None,
+                         config: Optional[dict] = None, stream=None) -> SparseHits:
+    """Pairs with score >= threshold (> 0).  Synchronises the stream (it must
+    read the hit count) and grows the hit buffers until every hit fits."""
+    lib = _native.load()
+    device = ref.mz.device if ref.mz is not None else qry.mz.device
+    s = _stream(device, stream)
+    ctx = _native.context(device.index)
+    cap = int(capacity) if capacity else max(1024, min(ref.n * qry.n, 1 << 22))
+    count = torch.zeros(1, dtype=torch.int64, device=device)
+    cfg = _cfg(config)
+    while True:
+        bufs = (torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.float32, device=device),
+                torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.uint8, device=device))
+        rc = lib.cms_cosine_greedy_sparse(
+            ctx.handle, ptr(ref.mz), ptr(ref.a), ptr(ref.b), ptr(ref.offsets), ref.n, ref.n_peaks,
+            ptr(qry.mz), ptr(qry.a), ptr(qry.b), ptr(qry.offsets), qry.n, qry.n_peaks,
+            float(tolerance), float(shift), int(match_limit), float(threshold),
+            *[ptr(b) for b in bufs], cap, ptr(count),
+            None if cfg is None else _ctypes_ref(cfg), stream_handle(s))
+        check(rc, "cms_cosine_greedy_sparse")
+        bits = ctx.take_device_error(stream_handle(s))  # synchronises s
+        if bits & _native.DEVERR_SPILL_OVERRUN and not (config or {}).get("mode") == 2:
+            config = dict(config or {})
+            config["mode"] = 2
+            cfg = _cfg(config)
+            continue
+        _raise_device_error(bits, "cms_cosine_greedy_sparse")
+        n = int(count.item())
+        if n <= cap:
+            return SparseHits(*bufs, n)
+        cap = n
+
+
+def fingerprint_matrix(measure: str, r_bits, r_valid, q_bits, q_valid, n_words: int, fill: float,
+                       *, out=None, stream=None):
+    """Fingerprint similarity [n_ref, n_q] float32 on the device."""
+    lib = _native.load()
+    device = r_bits.device
+    s = _stream(device, stream)
+    n_r, n_q = int(r_bits.shape[0]), int(q_bits.shape[0])
+    if out is None:
+        out = torch.empty((n_r, n_q), dtype=torch.float32, device=device)
+    rc = lib.cms_fingerprint(_native.FP_MEASURES[measure], ptr(r_bits), ptr(r_valid), n_r,
+                             ptr(q_bits), ptr(q_valid), n_q, int(n_words), float(fill), ptr(out),
+                             int(out.stride(0)), stream_handle(s))
+    check(rc, "cms_fingerprint")
+    return out

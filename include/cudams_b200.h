@@ -1,0 +1,197 @@
+/*
+ * cudams_b200.h -- C ABI of the B200 (sm_100a) pairwise mass-spectrum
+ * similarity library, libcudams_b200.so.
+ *
+ * The reference (tornikeo/cosine-similarity, package `cudams`) has no native
+ * library: its GPU work is one Numba-CUDA kernel and three PyTorch
+ * expressions called from two matchms plug-in classes.  This header is the
+ * boundary that replaces those device calls; the Python classes
+ * cudams.similarity.CudaCosineGreedy / CudaFingerprintSimilarity bind it with
+ * ctypes (cudams/_native.py).  Each entry point names the reference code it
+ * replaces.
+ *
+ * Conventions
+ *  - Every function returns CMS_OK (0) or a CMS_ERR_* code; the message of
+ *    the last failure on the calling thread is cms_last_error().  Nothing
+ *    throws across this boundary.
+ *  - All array arguments are DEVICE pointers owned by the caller, except
+ *    where a comment says "host".  `stream` is a cudaStream_t (NULL = legacy
+ *    default stream); work is enqueued asynchronously on it.
+ *  - Spectra are passed as CSR ("spectrum set"):
+ *        mz   float32 [n_peaks]   m/z, ascending within each spectrum
+ *        a    float64 [n_peaks]   mz^mz_power per peak, or NULL when
+ *                                 mz_power == 0 (then a == 1.0)
+ *        b    float64 [n_peaks]   intensity^intensity_power per peak
+ *        off  int64   [n + 1]     spectrum s owns peaks [off[s], off[s+1])
+ *    with at most CMS_MAX_PEAKS peaks per spectrum (peak indices are packed
+ *    in 16 bits, as the reference kernel packs them,
+ *    cudams/similarity/spectrum_similarity_functions.py:146).  The caller
+ *    applies the n_max_peaks truncation and the float32 rounding of m/z
+ *    (cudams/similarity/CudaCosineGreedy.py:74-85); cudams/packing.py does
+ *    both.
+ *  - Greedy-cosine outputs are three row-major [n_ref, ld] arrays, the three
+ *    planes of the reference's out[3, R, Q] (spectrum_similarity_functions.py
+ *    :59-61, :151, :261-262): score float32, matches int32, overflow uint8.
+ *  - A context (cms_ctx) owns the library's device scratch, tuning state and
+ *    error word.  One context per host thread; calls on one context must not
+ *    overlap in time on different streams.
+ */
+#ifndef CUDAMS_B200_H
+#define CUDAMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMS_OK 0
+#define CMS_ERR_INVALID 1     /* bad argument (null pointer, size, value)   */
+#define CMS_ERR_CUDA 2        /* a CUDA runtime call failed                  */
+#define CMS_ERR_UNSUPPORTED 3 /* valid but outside what this build supports  */
+#define CMS_ERR_NOMEM 4       /* device allocation failed                    */
+#define CMS_ERR_CAPACITY 5    /* sparse output buffer too small (see below)  */
+#define CMS_ERR_DEVICE 6      /* a kernel reported bad input (error word)    */
+
+#define CMS_MAX_PEAKS 65535
+
+#define CMS_FP_JACCARD 0
+#define CMS_FP_DICE 1
+#define CMS_FP_COSINE 2
+
+typedef struct cms_ctx cms_ctx;
+typedef struct cms_library cms_library;
+
+/* Library version as 10000*major + 100*minor + patch. */
+int cms_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* cms_last_error(void);
+
+/* Create / destroy a context bound to CUDA device `device`. */
+int cms_create(cms_ctx** out, int device);
+int cms_destroy(cms_ctx* ctx);
+
+/*
+ * Read and clear the context's device error word (synchronises `stream`).
+ * Kernels set bits in it instead of faulting when they meet input that
+ * breaks a precondition (a spectrum longer than CMS_MAX_PEAKS, a sparse
+ * spill list overrun).  *bits receives the word (host pointer).
+ */
+int cms_take_device_error(cms_ctx* ctx, uint32_t* bits, void* stream);
+
+/*
+ * Per-stage timing of the tiled path, for benchmarks.  When enabled, every
+ * cms_cosine_greedy* call records a CUDA event pair on its stream around each
+ * stage; cms_profile_read synchronises those events and returns, per stage,
+ * the summed device milliseconds and the number of kernel launches since the
+ * last reset (host arrays of CMS_PROFILE_STAGES entries; either may be NULL).
+ * Launch counts are kept even when timing is disabled.
+ * Stages: 0 validate+norms, 1 reference order, 2 query index, 3 join,
+ * 4 pair kernel.
+ */
+#define CMS_PROFILE_STAGES 5
+int cms_profile_enable(cms_ctx* ctx, int enable);
+int cms_profile_read(cms_ctx* ctx, double* stage_ms, int64_t* stage_launches, int reset);
+
+/*
+ * Plain greedy cosine: one (reference, query) pair per thread, the
+ * reference's own kernel design restated in CUDA C++ for sm_100a -- 512
+ * query threads per block over one reference spectrum, per-thread candidate
+ * arrays of match_limit entries, bottom-up merge sort, per-thread used-peak
+ * arrays cleared for every pair, query norm recomputed per pair.  Replaces
+ * cosine_greedy_kernel()/_kernel (spectrum_similarity_functions.py:12-278)
+ * as launched by CudaCosineGreedy.matrix (CudaCosineGreedy.py:149-181).
+ * It is the "plain" comparator of the benchmark and has the same numerics
+ * as cms_cosine_greedy (float64 keys, matchms ordering).
+ * match_limit <= 4096 and n_max_peaks <= 4096 (compile-time array sizes).
+ */
+int cms_cosine_greedy_plain(const float* ref_mz, const double* ref_a, const double* ref_b,
+                            const int64_t* ref_off, int64_t n_ref, const float* q_mz,
+                            const double* q_a, const double* q_b, const int64_t* q_off,
+                            int64_t n_q, double tolerance, double shift, int match_limit,
+                            int n_max_peaks, float* score, int32_t* matches, uint8_t* overflow,
+                            int64_t ld, void* stream);
+
+/*
+ * Tuning of the tiled path.  Zero in a field means "choose automatically".
+ *   tile_spectra   query spectra per indexed tile (<= 4096)
+ *   bucket_width   m/z width of one index bucket (>= tolerance)
+ *   n_buckets      buckets per tile (power of two)
+ *   mode           0 auto, 1 indexed join with pair spill, 2 pair kernel only
+ *   pair_threads   threads per CTA of the pair kernel (64..512, multiple of 32)
+ */
+typedef struct {
+    int32_t tile_spectra;
+    double bucket_width;
+    int32_t n_buckets;
+    int32_t mode;
+    int32_t pair_threads;
+} cms_cosine_config;
+
+/*
+ * Tiled greedy cosine, dense output.  Same contract and numerics as the
+ * reference's CudaCosineGreedy.matrix(array_type="numpy")
+ * (CudaCosineGreedy.py:107-205): for every (reference i, query j) writes
+ * score[i*ld+j], matches[i*ld+j], overflow[i*ld+j].
+ *   - window:  query peak matches reference peak iff
+ *              !(mz_q+shift > mz_r+tol) && !(mz_q+shift < mz_r-tol) (float64)
+ *   - key:     ((a_r*b_r)*a_q)*b_q (float64), sorted descending, ties to the
+ *              later-generated candidate (p_ref-major, p_query ascending)
+ *   - overflow = 1 when match_limit candidates were generated; only the
+ *              first match_limit (in generation order) take part.
+ * n_ref_peaks / n_q_peaks are the lengths of the peak arrays.  cfg may be
+ * NULL (automatic).  Internally: per-call query index (m/z buckets per tile
+ * of query spectra), a persistent warp-per-(reference, tile) join, and a
+ * CTA-per-pair kernel for pairs with many candidates.
+ */
+int cms_cosine_greedy(cms_ctx* ctx, const float* ref_mz, const double* ref_a, const double* ref_b,
+                      const int64_t* ref_off, int64_t n_ref, int64_t n_ref_peaks,
+                      const float* q_mz, const double* q_a, const double* q_b,
+                      const int64_t* q_off, int64_t n_q, int64_t n_q_peaks, double tolerance,
+                      double shift, int match_limit, float* score, int32_t* matches,
+                      uint8_t* overflow, int64_t ld, const cms_cosine_config* cfg, void* stream);
+
+/*
+ * Tiled greedy cosine, sparse output: every pair with score >= threshold
+ * (threshold > 0) is appended, in no particular order, to the hit arrays
+ * (hit_ref, hit_query int32; hit_score float32; hit_matches int32;
+ * hit_overflow uint8), at most `capacity` of them.  *hit_count (device
+ * int64, zeroed by the call) receives the number of qualifying pairs, which
+ * may exceed capacity: then only `capacity` hits were stored and the caller
+ * must retry with a larger buffer.  Replaces the array_type="sparse" branch
+ * of CudaCosineGreedy.matrix (CudaCosineGreedy.py:186-226), which builds the
+ * same (row, col, score, matches, overflow) tuples from `out[0] >= threshold`.
+ */
+int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                             const double* ref_b, const int64_t* ref_off, int64_t n_ref,
+                             int64_t n_ref_peaks, const float* q_mz, const double* q_a,
+                             const double* q_b, const int64_t* q_off, int64_t n_q,
+                             int64_t n_q_peaks, double tolerance, double shift, int match_limit,
+                             float threshold, int32_t* hit_ref, int32_t* hit_query,
+                             float* hit_score, int32_t* hit_matches, uint8_t* hit_overflow,
+                             int64_t capacity, int64_t* hit_count, const cms_cosine_config* cfg,
+                             void* stream);
+
+/*
+ * Fingerprint similarity on bit-packed fingerprints: n_words uint32 per
+ * row, bit k in word k/32 at bit k%32, unused high bits zero.  Writes
+ * out[i*ld + j] (float32) for every (reference i, query j):
+ *   CMS_FP_JACCARD  I / (a + b - I)      vector_similarity_functions.py:42-46
+ *   CMS_FP_DICE     2 * (I / (a + b))    vector_similarity_functions.py:87-90
+ *   CMS_FP_COSINE   I / sqrt(a * b)      vector_similarity_functions.py:116-118
+ * with I = popcount(r & q), a = popcount(r), b = popcount(q), each division
+ * and square root in IEEE float32, and 0/0 -> 0 (nan_to_num).  Rows whose
+ * valid flag is 0 (no fingerprint) give `fill` in all their pairs
+ * (CudaFingerprintSimilarity.py:147-177); valid arrays may be NULL (all
+ * valid).  n_words <= 1024.
+ */
+int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
+                    int64_t n_ref, const uint32_t* q_bits, const uint8_t* q_valid, int64_t n_q,
+                    int n_words, float fill, float* out, int64_t ld, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDAMS_B200_H */

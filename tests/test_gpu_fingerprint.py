@@ -1,0 +1,113 @@
+"""Fingerprint popcount kernel vs the oracle and the reference's own float32
+formulas: bit-exact."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_fingerprint_cases
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+MEASURES = ["jaccard", "dice", "cosine"]
+
+
+def _gpu(measure, rb, rv, qb, qv, n_words, fill):
+    import torch
+
+    from cudams import kernels
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda x: None if x is None else torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa
+    out = kernels.fingerprint_matrix(measure, t(rb), t(rv), t(qb), t(qv), n_words, fill)
+    return out.cpu().numpy()
+
+
+def _bits_equal(a, b):
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", golden_fingerprint_cases())
+@pytest.mark.parametrize("measure", MEASURES)
+def test_golden(cuda_device, name, measure):
+    from cudams.packing import pack_fingerprint_matrix
+
+    z = np.load(GOLDEN / f"fingerprint_{name}.npz")
+    rb, rv, _ = pack_fingerprint_matrix(z["ref"])
+    qb, qv, _ = pack_fingerprint_matrix(z["qry"])
+    got = _gpu(measure, rb, rv, qb, qv, rb.shape[1], np.nan)
+    _bits_equal(got, oracle.fingerprint(measure, rb, rv, qb, qv, rb.shape[1], np.nan))
+    if measure != "cosine":  # cosine: see test_oracle (torch-CPU sqrt quirk)
+        _bits_equal(got, z[measure])
+
+
+@pytest.mark.parametrize("measure", MEASURES)
+def test_vs_reference_formula_on_cuda(cuda_device, measure):
+    """The reference's own torch expressions (vector_similarity_functions.py
+    :42-46, :87-90, :116-118) run in float32 on the same B200: bit-exact."""
+    import torch
+
+    from cudams import synthetic
+    from cudams.packing import pack_fingerprint_matrix
+
+    rng = np.random.default_rng(1)
+    dens_r = rng.uniform(0.05, 0.15, 700)[:, None]
+    dens_q = rng.uniform(0.05, 0.15, 513)[:, None]
+    R = (rng.random((700, 2048)) < dens_r).astype(np.uint8)
+    Q = (rng.random((513, 2048)) < dens_q).astype(np.uint8)
+    R[3] = 0
+    Q[4] = 0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    refs = torch.from_numpy(R).to(dev).float()
+    ques = torch.from_numpy(Q).to(dev).float()
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        inter = refs @ ques.T
+        if measure == "jaccard":
+            union = refs.sum(1, keepdim=True) + ques.sum(1, keepdim=True).T
+            union -= inter
+            want = inter.div(union).nan_to_num()
+        elif measure == "dice":
+            union = refs.sum(1, keepdim=True).abs() + ques.sum(1, keepdim=True).abs().T
+            want = 2 * inter.div(union).nan_to_num()
+        else:
+            norm = refs.pow(2).sum(1, keepdim=True) @ ques.pow(2).sum(1, keepdim=True).T
+            want = inter.div(norm.sqrt()).nan_to_num(0)
+        want = want.cpu().numpy()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    rb, rv, _ = pack_fingerprint_matrix(R)
+    qb, qv, _ = pack_fingerprint_matrix(Q)
+    _bits_equal(_gpu(measure, rb, rv, qb, qv, rb.shape[1], np.nan), want)
+
+
+@pytest.mark.parametrize("n_bits", [1, 31, 32, 100, 2048, 2049, 4096, 32768])
+@pytest.mark.parametrize("measure", MEASURES)
+def test_sizes_and_masks(cuda_device, n_bits, measure):
+    from cudams.packing import pack_fingerprints
+
+    rng = np.random.default_rng(n_bits)
+    nr, nq = 131, 257
+    fps_r = [(rng.random(n_bits) < 0.3).astype(np.int8) if rng.random() > 0.1 else None
+             for _ in range(nr)]
+    fps_q = [(rng.random(n_bits) < 0.3).astype(np.int8) if rng.random() > 0.1 else None
+             for _ in range(nq)]
+    rb, rv, _ = pack_fingerprints(fps_r, n_bits)
+    qb, qv, _ = pack_fingerprints(fps_q, n_bits)
+    for fill in (np.nan, 0.0, -1.5):
+        got = _gpu(measure, rb, rv, qb, qv, rb.shape[1], fill)
+        _bits_equal(got, oracle.fingerprint(measure, rb, rv, qb, qv, rb.shape[1], fill))
+
+
+def test_large_symmetric(cuda_device):
+    """12k x 12k of the 2048-bit workload against itself: symmetric, diagonal 1,
+    and 20k sampled entries equal to the oracle."""
+    from cudams import synthetic
+
+    bits = synthetic.fingerprints(12000, seed=3)
+    got = _gpu("jaccard", bits, None, bits, None, bits.shape[1], np.nan)
+    _bits_equal(got, got.T.copy())
+    assert (np.diagonal(got) == 1.0).all()
+    rng = np.random.default_rng(0)
+    rows = rng.integers(0, 12000, 64)
+    want = oracle.fingerprint("jaccard", bits[rows], None, bits, None, bits.shape[1], np.nan)
+    _bits_equal(got[rows], want)
