@@ -261,7 +261,7 @@ def run_ours(args, world, rank, local):
     rd, qd = ref.to_device(dev), qry.to_device(dev)
     R, Q = ref.n, qry.n
     free, _ = torch.cuda.mem_get_info(dev)
-    rows = int(min(R, max(1024, (min(free * 0.6, 48e9)) // (Q * BYTES_PER_PAIR))))
+    rows = int(min(R, max(1024, (free * 0.6) // (Q * BYTES_PER_PAIR))))
     blocks = [(r0, min(R, r0 + rows)) for r0 in range(0, R, rows)]
     sub = [ref.subset(a, b).to_device(dev) if (a, b) != (0, R) else rd for a, b in blocks]
     out = (torch.empty((rows, Q), dtype=torch.float32, device=dev),

@@ -46,7 +46,7 @@ constexpr int kJoinWarps = 8;
 constexpr int kJoinThreads = kJoinWarps * 32;
 constexpr int kPool = 256;        // candidate pool entries per warp
 constexpr int kSmallRun = 16;     // longer runs go to the pair kernel
-constexpr int kMaxTile = 4096;    // max query spectra per tile (hasbits size)
+constexpr int kMaxTile = 4096;    // max query spectra per tile
 constexpr int kOrderClasses = 17; // log2 length classes (0..16)
 
 __device__ __forceinline__ double peak_a(const double* a, int64_t i) { return a ? a[i] : 1.0; }
@@ -123,6 +123,13 @@ __global__ void order_scatter_kernel(SpecSet S, const uint32_t* cls_count, uint3
 // ---------------------------------------------------------------------------
 // 4. tile index over the query side
 // ---------------------------------------------------------------------------
+// tile-stream entry: m/z, (query within tile << 16 | peak), intensity weight b
+struct __align__(16) Entry {
+    float mz;
+    uint32_t id;
+    double b;
+};
+
 struct IndexGeom {
     int tile;        // query spectra per tile
     int n_tiles;
@@ -198,7 +205,7 @@ __global__ void index_scan_kernel(IndexGeom g, uint32_t* cnt_cur, uint32_t* tab,
 }
 
 // warp per spectrum: scatter (m/z, q_local<<16 | peak) into the tile stream
-__global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, uint2* ent,
+__global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, Entry* ent,
                                      const uint32_t* bad) {
     if (*bad) return;
     const int lane = threadIdx.x & 31;
@@ -215,7 +222,11 @@ __global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, uint
             const float mz = B.mz[k];
             const unsigned bk = (unsigned)bucket_of((double)mz, g.inv_w) & mask;
             const uint32_t pos = atomicAdd(&c[bk], 1u);
-            ent[base + pos] = make_uint2(__float_as_uint(mz), (ql << 16) | (uint32_t)(k - lo));
+            Entry en;
+            en.mz = mz;
+            en.id = (ql << 16) | (uint32_t)(k - lo);
+            en.b = B.b[k];
+            ent[base + pos] = en;
         }
     }
 }
@@ -260,13 +271,15 @@ struct JoinParams {
     const double* snB;
     const int32_t* a_order;
     const uint32_t* tab;
-    const uint2* ent;
+    const Entry* ent;
     IndexGeom g;
     double tol;
     double shift;
     int match_limit;
-    int widen;  // bucket range widened by one on each side
-    float init_width_scale;  // initial sub-range width = clamp(scale / n_a_peaks)
+    int widen;               // bucket range widened by one on each side
+    float init_width_scale;  // first sub-range width = scale / n_A_peaks (0: whole tile)
+    int warp_smem_bytes;     // per-warp slice of dynamic shared memory
+    unsigned char* gpool;    // global pool extension, kGPool * 16 bytes per warp
     unsigned long long* work;
     SpillList spill;
     DenseOut dense;
@@ -275,34 +288,117 @@ struct JoinParams {
     const uint32_t* bad;
 };
 
-struct WarpSmem {
-    double key[kPool];
-    uint32_t gen[kPool];
-    uint32_t sk[kPool];           // (q_rel << 16) | slot, sorted
-    uint16_t run_start[kPool + 1];
-    float res_score[kPool];
-    int32_t res_matches[kPool];
-    uint32_t hasbits[kMaxTile / 32];
-    int n;
-    int n_runs;
+constexpr int kFetch = 4;  // work items taken per atomic
+constexpr int kPoolMax = 4096;             // candidates per sweep: smem pool + global extension
+constexpr int kGPool = kPoolMax - kPool;   // global extension entries per warp
+
+// A warp's candidate pool: the first kPool entries live in shared memory, the
+// rest in a per-warp slice of global scratch (L2-resident), so that a large
+// reference spectrum is swept once even when it has thousands of candidates
+// in a tile.  Slots are indices into the concatenation.
+struct Pool {
+    double* skey;
+    uint32_t* sgen;
+    uint16_t* scq;
+    uint16_t* sperm;
+    double* gkey;
+    uint32_t* ggen;
+    uint16_t* gcq;
+    uint16_t* gperm;
+    __device__ __forceinline__ double key(int i) const { return i < kPool ? skey[i] : gkey[i - kPool]; }
+    __device__ __forceinline__ uint32_t gen(int i) const { return i < kPool ? sgen[i] : ggen[i - kPool]; }
+    __device__ __forceinline__ int cq(int i) const { return i < kPool ? scq[i] : gcq[i - kPool]; }
+    __device__ __forceinline__ int perm(int i) const { return i < kPool ? sperm[i] : gperm[i - kPool]; }
+    __device__ __forceinline__ void put(int i, double k, uint32_t g, int q) const {
+        if (i < kPool) {
+            skey[i] = k;
+            sgen[i] = g;
+            scq[i] = (uint16_t)q;
+        } else {
+            gkey[i - kPool] = k;
+            ggen[i - kPool] = g;
+            gcq[i - kPool] = (uint16_t)q;
+        }
+    }
+    __device__ __forceinline__ void set_perm(int pos, int slot) const {
+        if (pos < kPool)
+            sperm[pos] = (uint16_t)slot;
+        else
+            gperm[pos - kPool] = (uint16_t)slot;
+    }
+    // a run's result, packed into the key slot of its first candidate
+    __device__ __forceinline__ void set_result(int i, int2 r) const {
+        if (i < kPool)
+            reinterpret_cast<int2*>(skey)[i] = r;
+        else
+            reinterpret_cast<int2*>(gkey)[i - kPool] = r;
+    }
+    __device__ __forceinline__ int2 result(int i) const {
+        return i < kPool ? reinterpret_cast<const int2*>(skey)[i]
+                         : reinterpret_cast<const int2*>(gkey)[i - kPool];
+    }
 };
 
-// bitonic sort of s[0..m) ascending, m a power of two, by one warp
-__device__ void warp_bitonic_u32(uint32_t* s, int m, int lane) {
-    for (int k = 2; k <= m; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = lane; i < m; i += 32) {
-                const int ixj = i ^ j;
-                if (ixj > i) {
-                    const uint32_t x = s[i], y = s[ixj];
-                    const bool up = (i & k) == 0;
-                    if (up ? (x > y) : (x < y)) {
-                        s[i] = y;
-                        s[ixj] = x;
-                    }
-                }
+// Per-warp shared-memory slice (offsets in bytes; the count array's length
+// depends on the tile size, so the slice size is computed at launch).
+//   ckey  double [kPool]   candidate key
+//   cgen  uint32 [kPool]   (p_ref << 16) | p_query
+//   cq    uint16 [kPool]   query index within the current sub-range
+//   perm  uint16 [kPool]   candidate slots grouped by query
+//   cnt   uint32 [tile/2+1] two 16-bit counters per word: per-query counts,
+//                          then (after the scan) starts, then (after the
+//                          scatter) ends of each query's run in perm
+//   n     int              candidates pushed in this sweep
+//   res   int2   [32]      per-lane staging of run results
+__host__ __device__ constexpr int warp_slice_bytes(int tile) {
+    return ((16 * kPool + 4 * (tile / 2 + 2) + 8 * 32 + 16) + 15) & ~15;
+}
+
+__device__ __forceinline__ unsigned cnt_get(const uint32_t* w, int q) {
+    return (w[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+}
+// counts never exceed kPool (< 2^16), so a half never carries into the other
+__device__ __forceinline__ unsigned cnt_inc(uint32_t* w, int q) {
+    const unsigned sh = (unsigned)(q & 1) * 16u;
+    return (atomicAdd(&w[q >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+
+// Greedy score of one query's candidate run perm[s..e), 2 <= e - s <= kSmallRun:
+// repeated selection in (key desc, gen desc) order, conflicts checked against
+// the accepted set.
+__device__ void resolve_run(const Pool& pool, int s, int e, double& score, int& matches) {
+    const int L = e - s;
+    unsigned done = 0, acc = 0;
+    score = 0.0;
+    matches = 0;
+    for (int it = 0; it < L; ++it) {
+        int best = -1;
+        double bk = 0.0;
+        uint32_t bg = 0;
+        for (int x = 0; x < L; ++x) {
+            if (done & (1u << x)) continue;
+            const int sl = pool.perm(s + x);
+            const double k = pool.key(sl);
+            const uint32_t gg = pool.gen(sl);
+            if (best < 0 || before(k, gg, bk, bg)) {
+                best = x;
+                bk = k;
+                bg = gg;
             }
-            __syncwarp();
+        }
+        done |= 1u << best;
+        bool ok = true;
+        for (unsigned m = acc; m; m &= m - 1) {
+            const uint32_t gx = pool.gen(pool.perm(s + __ffs(m) - 1));
+            if ((gx >> 16) == (bg >> 16) || (gx & 0xFFFFu) == (bg & 0xFFFFu)) {
+                ok = false;
+                break;
+            }
+        }
+        if (ok) {
+            acc |= 1u << best;
+            score = __dadd_rn(score, bk);
+            ++matches;
         }
     }
 }
@@ -312,26 +408,51 @@ __global__ void __launch_bounds__(kJoinThreads)
 join_kernel(JoinParams P) {
     if (*P.bad) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+    unsigned char* slice = smem_raw + (size_t)(threadIdx.x >> 5) * P.warp_smem_bytes;
+    double* ckey = reinterpret_cast<double*>(slice);
+    uint32_t* cgen = reinterpret_cast<uint32_t*>(slice + 8 * kPool);
+    uint16_t* cq = reinterpret_cast<uint16_t*>(slice + 12 * kPool);
+    uint16_t* perm = reinterpret_cast<uint16_t*>(slice + 14 * kPool);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(slice + 16 * kPool);
+    int* n_ptr = reinterpret_cast<int*>(slice + P.warp_smem_bytes - 16);
+    int2* res_pending = reinterpret_cast<int2*>(slice + P.warp_smem_bytes - 16 - 8 * 32);
+    Pool pool;
+    {
+        const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
+        unsigned char* g = P.gpool + gw * (size_t)kGPool * 16;
+        pool.skey = ckey;
+        pool.sgen = cgen;
+        pool.scq = cq;
+        pool.sperm = perm;
+        pool.gkey = reinterpret_cast<double*>(g);
+        pool.ggen = reinterpret_cast<uint32_t*>(g + 8 * kGPool);
+        pool.gcq = reinterpret_cast<uint16_t*>(g + 12 * kGPool);
+        pool.gperm = reinterpret_cast<uint16_t*>(g + 14 * kGPool);
+    }
+
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     const int64_t nA = P.A.n;
     const int64_t n_items = nA * (int64_t)P.g.n_tiles;
     const unsigned nbmask = (unsigned)(P.g.nb - 1);
+    const Entry* __restrict__ ent = P.ent;
+    const uint32_t* __restrict__ tab = P.tab;
 
     for (;;) {
-        unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(P.work, 1ull);
-        item = __shfl_sync(full, item, 0);
-        if ((int64_t)item >= n_items) break;
-        const int t = (int)((int64_t)item / nA);
-        const int a = P.a_order[(int64_t)item % nA];
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(P.work, (unsigned long long)kFetch);
+        base = __shfl_sync(full, base, 0);
+        if ((int64_t)base >= n_items) break;
+        for (int f = 0; f < kFetch && (int64_t)(base + f) < n_items; ++f) {
+        const int64_t item = (int64_t)base + f;
+        const int t = (int)(item / nA);
+        const int a = P.a_order[item % nA];
         const int64_t a0 = P.A.off[a];
         const int na = (int)(P.A.off[a + 1] - a0);
         const int b_begin = t * P.g.tile;
         const int tn = (int)min((int64_t)P.g.tile, P.B.n - b_begin);
         const int64_t tbase = P.B.off[b_begin];
-        const uint32_t* T = P.tab + (int64_t)t * (P.g.nb + 1);
+        const uint32_t* T = tab + (int64_t)t * (P.g.nb + 1);
         const double snA = P.snA[a];
 
         int width = tn;
@@ -341,9 +462,9 @@ join_kernel(JoinParams P) {
         while (range_lo < tn) {
             const int range_hi = min(range_lo + width, tn);
             const int rw = range_hi - range_lo;
-            // ---- sweep: collect candidates of (a, queries [range_lo, range_hi)) ----
-            for (int w = lane; w < (rw + 31) / 32; w += 32) W.hasbits[w] = 0u;
-            if (lane == 0) W.n = 0;
+            // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
+            for (int w = lane; w < rw / 2 + 1; w += 32) cnt[w] = 0u;
+            if (lane == 0) *n_ptr = 0;
             __syncwarp();
             for (int pc = 0; pc < na; pc += 32) {
                 const int p = pc + lane;
@@ -360,21 +481,34 @@ join_kernel(JoinParams P) {
                         slo = __dsub_rn(mz2_a, P.tol);
                         shi = __dadd_rn(mz2_a, P.tol);
                     }
-                    long long blo = bucket_of(slo, P.g.inv_w) - P.widen;
-                    long long bhi = bucket_of(shi, P.g.inv_w) + P.widen;
+                    const long long blo = bucket_of(slo, P.g.inv_w) - P.widen;
+                    const long long bhi = bucket_of(shi, P.g.inv_w) + P.widen;
+                    // the buckets of the window are one contiguous run of the
+                    // tile stream, or two when the hashed range wraps
+                    uint32_t r0b, r0e, r1b = 0, r1e = 0;
                     if (bhi - blo + 1 >= P.g.nb) {
-                        blo = 0;
-                        bhi = P.g.nb - 1;
+                        r0b = __ldg(&T[0]);
+                        r0e = __ldg(&T[P.g.nb]);
+                    } else {
+                        const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
+                        if (bl <= bh) {
+                            r0b = __ldg(&T[bl]);
+                            r0e = __ldg(&T[bh + 1]);
+                        } else {
+                            r0b = __ldg(&T[bl]);
+                            r0e = __ldg(&T[P.g.nb]);
+                            r1b = __ldg(&T[0]);
+                            r1e = __ldg(&T[bh + 1]);
+                        }
                     }
                     double wA = -1.0;  // a*b of this A peak, loaded on first candidate
-                    for (long long b = blo; b <= bhi; ++b) {
-                        const unsigned bk = (unsigned)b & nbmask;
-                        const uint32_t e0 = T[bk], e1 = T[bk + 1];
-                        for (uint32_t e = e0; e < e1; ++e) {
-                            const uint2 en = P.ent[tbase + e];
-                            const int bq = (int)(en.y >> 16);
+                    for (int part = 0; part < 2; ++part) {
+                        const uint32_t eb = part ? r1b : r0b, ee = part ? r1e : r0e;
+                        for (uint32_t e = eb; e < ee; ++e) {
+                            const Entry en = ent[tbase + e];
+                            const int bq = (int)(en.id >> 16);
                             if (bq < range_lo || bq >= range_hi) continue;
-                            const double mzB = (double)__uint_as_float(en.x);
+                            const double mzB = (double)en.mz;
                             bool match;
                             if (A_IS_REF) {
                                 const double mz2 = __dadd_rn(mzB, P.shift);
@@ -385,42 +519,41 @@ join_kernel(JoinParams P) {
                                 match = !(mz2_a > hi_b) && !(mz2_a < lo_b);
                             }
                             if (!match) continue;
-                            const int pB = (int)(en.y & 0xFFFFu);
-                            const int64_t gB = P.B.off[b_begin + bq] + pB;
+                            const int pB = (int)(en.id & 0xFFFFu);
+                            const double aB =
+                                P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
                             if (wA < 0.0) wA = __dmul_rn(peak_a(P.A.a, a0 + p), P.A.b[a0 + p]);
                             double key;
                             uint32_t gen;
                             if (A_IS_REF) {
-                                key = __dmul_rn(__dmul_rn(wA, peak_a(P.B.a, gB)), P.B.b[gB]);
+                                key = __dmul_rn(__dmul_rn(wA, aB), en.b);
                                 gen = ((uint32_t)p << 16) | (uint32_t)pB;
                             } else {
-                                const double wB = __dmul_rn(peak_a(P.B.a, gB), P.B.b[gB]);
+                                const double wB = __dmul_rn(aB, en.b);
                                 key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + p)),
                                                 P.A.b[a0 + p]);
                                 gen = ((uint32_t)pB << 16) | (uint32_t)p;
                             }
-                            const int slot = atomicAdd(&W.n, 1);
-                            if (slot < kPool) {
+                            const int slot = atomicAdd(n_ptr, 1);
+                            if (slot < kPoolMax) {
                                 const int qr = bq - range_lo;
-                                W.key[slot] = key;
-                                W.gen[slot] = gen;
-                                W.sk[slot] = ((uint32_t)qr << 16) | (uint32_t)slot;
-                                atomicOr(&W.hasbits[qr >> 5], 1u << (qr & 31));
+                                pool.put(slot, key, gen, qr);
+                                cnt_inc(cnt, qr);
                             }
                         }
                     }
                 }
                 __syncwarp();
-                const int n_now = *(volatile int*)&W.n;
+                const int n_now = *(volatile int*)n_ptr;
                 __syncwarp();
-                if (n_now > kPool) break;
+                if (n_now > kPoolMax) break;
             }
             __syncwarp();
-            const int n = *(volatile int*)&W.n;
-            if (n > kPool) {
+            const int n = *(volatile int*)n_ptr;
+            if (n > kPoolMax) {
                 if (rw > 1) {
                     // too many candidates for one pool: retry a narrower range
-                    width = max(1, (int)((long long)rw * kPool / (2LL * n)));
+                    width = max(1, (int)((long long)rw * kPoolMax / (2LL * n)));
                     width = min(width, rw / 2 > 0 ? rw / 2 : 1);
                     __syncwarp();
                     continue;
@@ -443,134 +576,154 @@ join_kernel(JoinParams P) {
                 continue;
             }
 
-            // ---- group the pool by query: sort (q_rel, slot) ----
-            if (n > 1) {
-                int m = 2;
-                while (m < n) m <<= 1;
-                for (int i = n + lane; i < m; i += 32) W.sk[i] = 0xffffffffu;
+            if (n > 0) {
+                // ---- counting sort of the pool by query ----
+                // exclusive scan of the per-query counts, in place (words of two)
+                const int nw = rw / 2 + 1;
+                const int per = (nw + 31) / 32;
+                const int w0 = min(nw, lane * per), w1 = min(nw, w0 + per);
+                unsigned local = 0;
+                for (int w = w0; w < w1; ++w) {
+                    const uint32_t v = cnt[w];
+                    local += (v & 0xFFFFu) + (v >> 16);
+                }
+                unsigned incl = local;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const unsigned u = __shfl_up_sync(full, incl, d);
+                    if (lane >= d) incl += u;
+                }
+                unsigned run = incl - local;
+                for (int w = w0; w < w1; ++w) {
+                    const uint32_t v = cnt[w];
+                    const unsigned lo = v & 0xFFFFu;
+                    cnt[w] = run | ((run + lo) << 16);
+                    run += lo + (v >> 16);
+                }
                 __syncwarp();
-                warp_bitonic_u32(W.sk, m, lane);
+                // scatter: the counters become run ends
+                for (int sl = lane; sl < n; sl += 32) pool.set_perm(cnt_inc(cnt, pool.cq(sl)), sl);
+                __syncwarp();
             }
-            // run starts
+
+            // ---- resolve each query's run, compactly: one lane per run ----
+            // Runs are contiguous in perm and ordered by query; a run starts
+            // where the query index changes.  The result of a run is packed
+            // into the ckey slot of its first candidate: (score f32 bits,
+            // matches), matches = -1 for a pair sent to the pair kernel.
             int n_runs = 0;
             for (int c = 0; c < n; c += 32) {
                 const int i = c + lane;
-                bool start = false;
-                if (i < n) start = (i == 0) || ((W.sk[i] >> 16) != (W.sk[i - 1] >> 16));
-                const unsigned bal = __ballot_sync(full, start);
-                if (start) W.run_start[n_runs + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
+                bool st = false;
+                int q_i = 0;
+                if (i < n) {
+                    q_i = pool.cq(pool.perm(i));
+                    st = (i == 0) || (pool.cq(pool.perm(i - 1)) != q_i);
+                }
+                const unsigned bal = __ballot_sync(full, st);
                 n_runs += __popc(bal);
-            }
-            if (lane == 0) W.run_start[n_runs] = (uint16_t)n;
-            __syncwarp();
-
-            // ---- resolve each run (one lane per query) ----
-            for (int r = lane; r < n_runs; r += 32) {
-                const int s = W.run_start[r], e = W.run_start[r + 1];
-                const int L = e - s;
-                const int qr = (int)(W.sk[s] >> 16);
-                const int bq = b_begin + range_lo + qr;
-                const int rr = A_IS_REF ? a : bq, qq = A_IS_REF ? bq : a;
-                float sc;
-                int mt;
-                if (L >= P.match_limit || L > kSmallRun) {
-                    spill_push(P.spill, rr, qq, P.err);
-                    sc = __int_as_float(0x7fc00000);
-                    mt = -1;
-                } else {
-                    double score = 0.0;
-                    int matches = 0;
-                    if (L == 1) {
-                        score = W.key[W.sk[s] & 0xFFFFu];
-                        matches = 1;
+                // lanes starting a run resolve it now (the run ends at the next
+                // query's end counter)
+                if (st) {
+                    const int e = (int)cnt_get(cnt, q_i);
+                    const int L = e - i;
+                    const int bq = b_begin + range_lo + q_i;
+                    float sc;
+                    int mt;
+                    if (L >= P.match_limit || L > kSmallRun) {
+                        spill_push(P.spill, A_IS_REF ? a : bq, A_IS_REF ? bq : a, P.err);
+                        sc = __int_as_float(0x7fc00000);
+                        mt = -1;
                     } else {
-                        // selection in greedy order; conflicts against accepted
-                        unsigned done = 0, acc = 0;
-                        for (int it = 0; it < L; ++it) {
-                            int best = -1;
-                            double bk = 0.0;
-                            uint32_t bg = 0;
-                            for (int x = 0; x < L; ++x) {
-                                if (done & (1u << x)) continue;
-                                const int sl = (int)(W.sk[s + x] & 0xFFFFu);
-                                const double k = W.key[sl];
-                                const uint32_t gg = W.gen[sl];
-                                if (best < 0 || before(k, gg, bk, bg)) {
-                                    best = x;
-                                    bk = k;
-                                    bg = gg;
-                                }
-                            }
-                            done |= 1u << best;
-                            bool ok = true;
-                            for (unsigned m2 = acc; m2; m2 &= m2 - 1) {
-                                const int x = __ffs(m2) - 1;
-                                const uint32_t gx = W.gen[W.sk[s + x] & 0xFFFFu];
-                                if ((gx >> 16) == (bg >> 16) || (gx & 0xFFFFu) == (bg & 0xFFFFu)) {
-                                    ok = false;
-                                    break;
-                                }
-                            }
-                            if (ok) {
-                                acc |= 1u << best;
-                                score = __dadd_rn(score, bk);
-                                ++matches;
-                            }
+                        double score;
+                        if (L == 1) {
+                            score = pool.key(pool.perm(i));
+                            mt = 1;
+                        } else {
+                            resolve_run(pool, i, e, score, mt);
+                        }
+                        const double snB = P.snB[bq];
+                        sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
+                                                              : __dmul_rn(snB, snA));
+                    }
+                    // lanes of other runs may still be reading their own slots
+                    // only; this slot belongs to this run
+                    res_pending[lane] = make_int2(__float_as_int(sc), mt);
+                }
+                __syncwarp();
+                if (st) pool.set_result(pool.perm(i), res_pending[lane]);
+                __syncwarp();
+            }
+            (void)n_runs;
+
+            // ---- write the results ----
+            if (!SPARSE) {
+                // dense row segment out[a, b_begin + range_lo ...): every query
+                // of the range, zeros where there is no candidate; 4 queries per
+                // lane with 16-byte streaming stores when aligned
+                const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
+                auto result_of = [&](int qr, float& sc, int& mt) {
+                    sc = 0.f;
+                    mt = 0;
+                    if (n > 0) {
+                        const int e = (int)cnt_get(cnt, qr);
+                        const int s = qr > 0 ? (int)cnt_get(cnt, qr - 1) : 0;
+                        if (e > s) {
+                            const int2 r = pool.result(pool.perm(s));
+                            sc = __int_as_float(r.x);
+                            mt = r.y;
                         }
                     }
-                    const double snB = P.snB[bq];
-                    const double denom = A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA);
-                    sc = (float)__ddiv_rn(score, denom);
-                    mt = matches;
+                };
+                int qv = 0;
+                if ((row & 3) == 0 && (P.dense.ld & 3) == 0) {
+                    for (; qv + 128 <= rw; qv += 128) {
+                        const int q0 = qv + 4 * lane;
+                        float4 s4;
+                        int4 m4;
+                        result_of(q0 + 0, s4.x, m4.x);
+                        result_of(q0 + 1, s4.y, m4.y);
+                        result_of(q0 + 2, s4.z, m4.z);
+                        result_of(q0 + 3, s4.w, m4.w);
+                        __stcs(reinterpret_cast<float4*>(P.dense.score + row + q0), s4);
+                        __stcs(reinterpret_cast<int4*>(P.dense.matches + row + q0), m4);
+                        __stcs(reinterpret_cast<uchar4*>(P.dense.overflow + row + q0),
+                               make_uchar4(0, 0, 0, 0));
+                    }
                 }
-                W.res_score[r] = sc;
-                W.res_matches[r] = mt;
-            }
-            __syncwarp();
-
-            // ---- write results ----
-            if (!SPARSE) {
-                // dense row segment out[a, b_begin + range_lo ...), coalesced
-                int rank_base = 0;
-                const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
+                for (int qr = qv + lane; qr < rw; qr += 32) {
+                    float sc;
+                    int mt;
+                    result_of(qr, sc, mt);
+                    __stcs(&P.dense.score[row + qr], sc);
+                    __stcs(&P.dense.matches[row + qr], mt);
+                    __stcs(&P.dense.overflow[row + qr], (unsigned char)0);
+                }
+            } else if (n > 0) {
                 for (int c = 0; c < rw; c += 32) {
                     const int qr = c + lane;
-                    const uint32_t word = W.hasbits[c >> 5];
-                    if (qr < rw) {
-                        float sc = 0.f;
-                        int mt = 0;
-                        if ((word >> lane) & 1u) {
-                            const int rk = rank_base + __popc(word & ((1u << lane) - 1u));
-                            sc = W.res_score[rk];
-                            mt = W.res_matches[rk];
-                        }
-                        // a spilled pair gets (NaN, -1, 0) here; the pair kernel,
-                        // launched after this one on the same stream, overwrites it
-                        P.dense.score[row + qr] = sc;
-                        P.dense.matches[row + qr] = mt;
-                        P.dense.overflow[row + qr] = 0;
-                    }
-                    rank_base += __popc(word);
-                }
-            } else {
-                for (int c = 0; c < n_runs; c += 32) {
-                    const int r = c + lane;
                     bool hit = false;
                     float sc = 0.f;
-                    int mt = 0, bq = 0;
-                    if (r < n_runs) {
-                        sc = W.res_score[r];
-                        mt = W.res_matches[r];
-                        bq = b_begin + range_lo + (int)(W.sk[W.run_start[r]] >> 16);
-                        hit = mt >= 0 && sc >= P.sparse.threshold;
+                    int mt = 0;
+                    const int bq = b_begin + range_lo + qr;
+                    if (qr < rw) {
+                        const int e = (int)cnt_get(cnt, qr);
+                        const int s = qr > 0 ? (int)cnt_get(cnt, qr - 1) : 0;
+                        if (e > s) {
+                            const int2 r = pool.result(pool.perm(s));
+                            sc = __int_as_float(r.x);
+                            mt = r.y;
+                            hit = mt >= 0 && sc >= P.sparse.threshold;
+                        }
                     }
                     const unsigned bal = __ballot_sync(full, hit);
                     if (bal) {
-                        unsigned long long base = 0;
-                        if (lane == 0) base = atomicAdd(P.sparse.count, (unsigned long long)__popc(bal));
-                        base = __shfl_sync(full, base, 0);
+                        unsigned long long hb = 0;
+                        if (lane == 0)
+                            hb = atomicAdd(P.sparse.count, (unsigned long long)__popc(bal));
+                        hb = __shfl_sync(full, hb, 0);
                         if (hit) {
-                            const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
+                            const unsigned long long pos = hb + __popc(bal & ((1u << lane) - 1u));
                             if (pos < (unsigned long long)P.sparse.capacity) {
                                 P.sparse.r[pos] = A_IS_REF ? a : bq;
                                 P.sparse.q[pos] = A_IS_REF ? bq : a;
@@ -584,9 +737,10 @@ join_kernel(JoinParams P) {
             }
             __syncwarp();
             range_lo = range_hi;
-            if (n < kPool / 4) width = min(tn, width * 2);
+            if (n < kPoolMax / 4) width = min(tn, width * 2);
         }
         __syncwarp();
+        }
     }
 }
 
@@ -885,6 +1039,10 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
 
     // ---- scratch layout ----
     const int64_t nR = args.ref.n, nQ = args.qry.n;
+    // global pool extension for every warp the join grid can hold (at most
+    // 64 warps per SM are resident)
+    const size_t gpool_warps = (size_t)ctx->sm_count * 64;
+    const size_t gpool_bytes = gpool_warps * (size_t)kGPool * 16;
     size_t need = 0;
     need += bump_size(64 * sizeof(uint64_t));            // flags, counters
     need += bump_size(nR * sizeof(double)) + bump_size(nQ * sizeof(double));
@@ -892,8 +1050,9 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         need += bump_size(nR * sizeof(int32_t));
         need += bump_size((size_t)p.n_tiles * (p.nb + 1) * sizeof(uint32_t));
         need += bump_size((size_t)p.n_tiles * p.nb * sizeof(uint32_t));
-        need += bump_size((size_t)std::max<int64_t>(1, args.qry.n_peaks) * sizeof(uint2));
+        need += bump_size((size_t)std::max<int64_t>(1, args.qry.n_peaks) * sizeof(Entry));
         need += bump_size((size_t)p.spill_cap * sizeof(int2));
+        need += bump_size(gpool_bytes);
     }
     need += 4096;
     rc = arena_reserve(ctx, ctx->scratch, need, s);
@@ -971,8 +1130,9 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     int32_t* order = bp.take<int32_t>(nR);
     uint32_t* tab = bp.take<uint32_t>((size_t)p.n_tiles * (p.nb + 1));
     uint32_t* cur = bp.take<uint32_t>((size_t)p.n_tiles * p.nb);
-    uint2* ent = bp.take<uint2>((size_t)std::max<int64_t>(1, args.qry.n_peaks));
+    Entry* ent = bp.take<Entry>((size_t)std::max<int64_t>(1, args.qry.n_peaks));
     int2* spill = bp.take<int2>(p.spill_cap);
+    unsigned char* gpool = bp.take<unsigned char>(gpool_bytes);
 
     {
         StageScope sc(ctx, 1, 2, s);
@@ -1005,13 +1165,20 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.match_limit = args.match_limit;
     jp.widen = args.shift != 0.0 ? 1 : 0;
     jp.init_width_scale = 0.f;
+    if (cfg && cfg->cand_per_pair > 0.0 && args.ref.n > 0) {
+        // expected candidates of (A spectrum with n peaks, w queries) ~ n*w*lambda
+        const double mean_na = (double)args.ref.n_peaks / (double)args.ref.n;
+        const double lambda = cfg->cand_per_pair / std::max(1.0, mean_na);
+        jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
+    }
+    jp.warp_smem_bytes = warp_slice_bytes(p.tile);
     jp.work = work_join;
     jp.spill = SpillList{spill, spill_count, p.spill_cap};
     jp.dense = pp.dense;
     jp.sparse = pp.sparse;
     jp.err = ctx->err_word;
     jp.bad = bad;
-    const size_t join_smem = sizeof(WarpSmem) * kJoinWarps;
+    const size_t join_smem = (size_t)warp_slice_bytes(p.tile) * kJoinWarps;
     int join_blocks_per_sm = 1;
     {
     StageScope sc(ctx, 3, 1, s);
@@ -1019,15 +1186,21 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         set_func_smem(join_kernel<true, true>, join_smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, true>,
                                                       kJoinThreads, join_smem);
-        join_kernel<true, true><<<ctx->sm_count * std::max(1, join_blocks_per_sm), kJoinThreads,
-                                  join_smem, s>>>(jp);
     } else {
         set_func_smem(join_kernel<true, false>, join_smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, false>,
                                                       kJoinThreads, join_smem);
-        join_kernel<true, false><<<ctx->sm_count * std::max(1, join_blocks_per_sm), kJoinThreads,
-                                   join_smem, s>>>(jp);
     }
+    const int join_grid = ctx->sm_count * std::max(1, join_blocks_per_sm);
+    jp.gpool = gpool;
+    if ((size_t)join_grid * kJoinWarps > gpool_warps) {
+        set_error("cms_cosine_greedy: join grid larger than its scratch");
+        return CMS_ERR_CUDA;
+    }
+    if (sparse)
+        join_kernel<true, true><<<join_grid, kJoinThreads, join_smem, s>>>(jp);
+    else
+        join_kernel<true, false><<<join_grid, kJoinThreads, join_smem, s>>>(jp);
     }
     CMS_CUDA_TRY(cudaGetLastError());
 

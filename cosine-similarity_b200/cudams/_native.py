@@ -78,6 +78,7 @@ class CosineConfig(ctypes.Structure):
         ("n_buckets", c_int32),
         ("mode", c_int32),
         ("pair_threads", c_int32),
+        ("cand_per_pair", c_double),
     ]
 
 

@@ -78,7 +78,7 @@ def heuristic_config(stats: WorkloadStats, n_q: int) -> dict:
     tile = max(32, min(4096, tile))
     tile = (tile + 31) // 32 * 32
     tile = min(tile, max(32, (n_q + 31) // 32 * 32))
-    return {"mode": 1, "tile_spectra": tile}
+    return {"mode": 1, "tile_spectra": tile, "cand_per_pair": float(stats.cand_per_pair)}
 
 
 class Tuner:

@@ -89,6 +89,21 @@ class PackedSpectra:
                                               up(self.offsets), self.n, self.n_peaks)
         return self._device[key]
 
+    def truncate(self, n_max_peaks: Optional[int]) -> "PackedSpectra":
+        """Keep the first `n_max_peaks` peaks of every spectrum (self if none is longer)."""
+        if n_max_peaks is None or self.n == 0:
+            return self
+        lengths = self.lengths
+        if lengths.max(initial=0) <= n_max_peaks:
+            return self
+        keep = np.minimum(lengths, int(n_max_peaks))
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        np.cumsum(keep, out=off[1:])
+        seg = np.repeat(np.arange(self.n), keep)
+        idx = self.offsets[:-1][seg] + (np.arange(off[-1]) - off[:-1][seg])
+        return PackedSpectra(self.mz[idx], None if self.a is None else self.a[idx], self.b[idx],
+                             off, self.mz_power, self.intensity_power, int(n_max_peaks))
+
     def subset(self, start: int, stop: int) -> "PackedSpectra":
         """Spectra [start, stop) as a new packed set (peaks re-based to 0)."""
         lo, hi = int(self.offsets[start]), int(self.offsets[stop])

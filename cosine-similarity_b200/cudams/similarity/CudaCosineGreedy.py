@@ -102,7 +102,7 @@ class CudaCosineGreedy(BaseSimilarity):
             if (spectra.mz_power != float(self.mz_power)
                     or spectra.intensity_power != float(self.int_power)):
                 raise ValueError("PackedSpectra was packed with other mz/intensity powers")
-            return spectra
+            return spectra.truncate(self.n_max_peaks)
         return pack_spectra(spectra, self.n_max_peaks, self.mz_power, self.int_power)
 
     def _spectra_peaks_to_tensor(self, spectra: list):

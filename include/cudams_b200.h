@@ -120,6 +120,9 @@ int cms_cosine_greedy_plain(const float* ref_mz, const double* ref_a, const doub
  *   n_buckets      buckets per tile (power of two)
  *   mode           0 auto, 1 indexed join with pair spill, 2 pair kernel only
  *   pair_threads   threads per CTA of the pair kernel (64..512, multiple of 32)
+ *   cand_per_pair  expected candidates per pair (e.g. sampled on the host);
+ *                  sizes the first query sub-range of large spectra so the
+ *                  join's candidate pool rarely overflows (0: unknown)
  */
 typedef struct {
     int32_t tile_spectra;
@@ -127,6 +130,7 @@ typedef struct {
     int32_t n_buckets;
     int32_t mode;
     int32_t pair_threads;
+    double cand_per_pair;
 } cms_cosine_config;
 
 /*

@@ -53,6 +53,18 @@ def test_pack_rejects_unsorted_and_nonfinite():
         pack_spectra([(np.arange(70000.0), np.ones(70000))], n_max_peaks=None)
 
 
+def test_truncate_equals_packing_truncation():
+    from cudams import synthetic
+    from cudams.packing import pack_csr
+
+    p = synthetic.uniform_spectra(60, seed=2)
+    t = p.truncate(37)
+    want = pack_csr(p.mz, p.b, p.offsets, 37)
+    for f in ("mz", "b", "offsets"):
+        np.testing.assert_array_equal(getattr(t, f), getattr(want, f))
+    assert p.truncate(5000) is p
+
+
 def test_subset():
     from cudams import synthetic
 
