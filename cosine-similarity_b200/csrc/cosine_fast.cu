@@ -45,7 +45,7 @@ namespace {
 constexpr int kJoinWarps = 8;
 constexpr int kJoinThreads = kJoinWarps * 32;
 constexpr int kPool = 256;        // candidate pool entries per warp
-constexpr int kSmallRun = 16;     // longer runs go to the pair kernel
+constexpr int kLongRun = 32;      // longer runs go to the pair kernel
 constexpr int kMaxTile = 4096;    // max query spectra per tile
 constexpr int kOrderClasses = 17; // log2 length classes (0..16)
 
@@ -137,8 +137,12 @@ struct IndexGeom {
     double inv_w;    // 1 / bucket width
 };
 
-__device__ __forceinline__ long long bucket_of(double x, double inv_w) {
-    return (long long)floor(x * inv_w);
+// Bucket of an m/z value: floor(mz / width), hashed modulo nb by the caller.
+// Monotone non-decreasing in mz (one float64 multiply, then round down), so
+// every entry inside [L, H] falls in a bucket of [bucket_of(L), bucket_of(H)].
+// (float64 keeps one bucket per width even when mz / width exceeds 2^24.)
+__device__ __forceinline__ long long bucket_of(float x, double inv_w) {
+    return __double2ll_rd(__dmul_rn((double)x, inv_w));
 }
 
 // warp per spectrum: histogram of (tile, bucket)
@@ -153,7 +157,7 @@ __global__ void index_count_kernel(SpecSet B, IndexGeom g, uint32_t* cnt, const 
         const int64_t lo = B.off[s], hi = B.off[s + 1];
         uint32_t* c = cnt + t * (int64_t)g.nb;
         for (int64_t k = lo + lane; k < hi; k += 32) {
-            const unsigned bk = (unsigned)bucket_of((double)B.mz[k], g.inv_w) & mask;
+            const unsigned bk = (unsigned)bucket_of(B.mz[k], g.inv_w) & mask;
             atomicAdd(&c[bk], 1u);
         }
     }
@@ -220,7 +224,7 @@ __global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, Entr
         uint32_t* c = cur + t * (int64_t)g.nb;
         for (int64_t k = lo + lane; k < hi; k += 32) {
             const float mz = B.mz[k];
-            const unsigned bk = (unsigned)bucket_of((double)mz, g.inv_w) & mask;
+            const unsigned bk = (unsigned)bucket_of(mz, g.inv_w) & mask;
             const uint32_t pos = atomicAdd(&c[bk], 1u);
             Entry en;
             en.mz = mz;
@@ -276,7 +280,6 @@ struct JoinParams {
     double tol;
     double shift;
     int match_limit;
-    int widen;               // bucket range widened by one on each side
     float init_width_scale;  // first sub-range width = scale / n_A_peaks (0: whole tile)
     int warp_smem_bytes;     // per-warp slice of dynamic shared memory
     unsigned char* gpool;    // global pool extension, kGPool * 16 bytes per warp
@@ -350,8 +353,13 @@ struct Pool {
 //                          scatter) ends of each query's run in perm
 //   n     int              candidates pushed in this sweep
 //   res   int2   [32]      per-lane staging of run results
+//   long  uint16 [kLongRuns] starts of runs longer than 2 (resolved by the warp)
+constexpr int kLongRuns = 64;
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
-    return ((16 * kPool + 4 * (tile / 2 + 2) + 8 * 32 + 16) + 15) & ~15;
+    // counters: tile/2 + 1 words are used; the 16-byte zeroing may touch up
+    // to tile/2 + 5, so round that up to whole uint4s
+    return ((16 * kPool + 4 * (((tile / 2 + 5) + 3) & ~3) + 2 * kLongRuns + 8 * 32 + 16) + 15) &
+           ~15;
 }
 
 __device__ __forceinline__ unsigned cnt_get(const uint32_t* w, int q) {
@@ -363,48 +371,70 @@ __device__ __forceinline__ unsigned cnt_inc(uint32_t* w, int q) {
     return (atomicAdd(&w[q >> 1], 1u << sh) >> sh) & 0xFFFFu;
 }
 
-// Greedy score of one query's candidate run perm[s..e), 2 <= e - s <= kSmallRun:
-// repeated selection in (key desc, gen desc) order, conflicts checked against
-// the accepted set.
-__device__ void resolve_run(const Pool& pool, int s, int e, double& score, int& matches) {
-    const int L = e - s;
-    unsigned done = 0, acc = 0;
-    score = 0.0;
-    matches = 0;
-    for (int it = 0; it < L; ++it) {
-        int best = -1;
-        double bk = 0.0;
-        uint32_t bg = 0;
-        for (int x = 0; x < L; ++x) {
-            if (done & (1u << x)) continue;
-            const int sl = pool.perm(s + x);
-            const double k = pool.key(sl);
-            const uint32_t gg = pool.gen(sl);
-            if (best < 0 || before(k, gg, bk, bg)) {
-                best = x;
-                bk = k;
-                bg = gg;
-            }
-        }
-        done |= 1u << best;
-        bool ok = true;
-        for (unsigned m = acc; m; m &= m - 1) {
-            const uint32_t gx = pool.gen(pool.perm(s + __ffs(m) - 1));
-            if ((gx >> 16) == (bg >> 16) || (gx & 0xFFFFu) == (bg & 0xFFFFu)) {
-                ok = false;
-                break;
-            }
-        }
-        if (ok) {
-            acc |= 1u << best;
-            score = __dadd_rn(score, bk);
-            ++matches;
-        }
+// Exact float32 window of one sweeping peak.
+//
+// The float64 test of the reference (query peak y matches reference peak x iff
+// !(y+shift > x+tol) && !(y+shift < x-tol)) is, for a fixed sweeping peak, a
+// conjunction of a predicate non-decreasing in the indexed peak's m/z and one
+// non-increasing in it.  So the float32 values it accepts form one interval
+// [L, H] of float32 numbers.  It is found once per sweeping peak by rounding
+// an estimate and stepping with nextafterf until the float64 predicates flip;
+// each entry is then tested with two float32 compares, with exactly the same
+// outcome as the float64 test.  The estimate is within an ulp or two; the
+// step loops are capped, and a peak that does not converge (non-finite input)
+// gets an empty window and an error flag.
+template <bool A_IS_REF, bool NOSHIFT>
+struct Window {
+    // A_IS_REF: x = sweeping reference peak; lo/hi = x -+ tol
+    // else:     c = sweeping query peak + shift
+    __device__ __forceinline__ static bool not_below(float y, double lo, double c, double tol,
+                                                     double shift) {
+        if (A_IS_REF) return !(__dadd_rn((double)y, shift) < lo);
+        return !(c > __dadd_rn((double)y, tol));
     }
-}
+    __device__ __forceinline__ static bool not_above(float y, double hi, double c, double tol,
+                                                     double shift) {
+        if (A_IS_REF) return !(__dadd_rn((double)y, shift) > hi);
+        return !(c < __dsub_rn((double)y, tol));
+    }
+    __device__ static bool bounds(float mzA, double tol, double shift, float& L, float& H) {
+        const double x = (double)mzA;
+        if (A_IS_REF && NOSHIFT) {
+            // y (float32, exact in float64) is accepted iff lo <= y <= hi: the
+            // interval ends are lo rounded up and hi rounded down to float32
+            L = __double2float_ru(__dsub_rn(x, tol));
+            H = __double2float_rd(__dadd_rn(x, tol));
+            return isfinite(L) && isfinite(H);
+        }
+        double lo = 0.0, hi = 0.0, c = 0.0, el, eh;
+        if (A_IS_REF) {
+            lo = __dsub_rn(x, tol);
+            hi = __dadd_rn(x, tol);
+            el = __dsub_rn(lo, shift);
+            eh = __dsub_rn(hi, shift);
+        } else {
+            c = __dadd_rn(x, shift);
+            el = __dsub_rn(c, tol);
+            eh = __dadd_rn(c, tol);
+        }
+        float l = __double2float_rd(el), h = __double2float_ru(eh);
+        int k = 0;
+        for (; k < 16 && !not_below(l, lo, c, tol, shift); ++k) l = nextafterf(l, INFINITY);
+        for (; k < 32 && not_below(nextafterf(l, -INFINITY), lo, c, tol, shift); ++k)
+            l = nextafterf(l, -INFINITY);
+        for (; k < 48 && !not_above(h, hi, c, tol, shift); ++k) h = nextafterf(h, -INFINITY);
+        for (; k < 64 && not_above(nextafterf(h, INFINITY), hi, c, tol, shift); ++k)
+            h = nextafterf(h, INFINITY);
+        const bool ok = k < 64 && isfinite(l) && isfinite(h) && not_below(l, lo, c, tol, shift) &&
+                        not_above(h, hi, c, tol, shift);
+        L = l;
+        H = h;
+        return ok;
+    }
+};
 
-template <bool A_IS_REF, bool SPARSE>
-__global__ void __launch_bounds__(kJoinThreads)
+template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
+__global__ void __launch_bounds__(kJoinThreads, 4)
 join_kernel(JoinParams P) {
     if (*P.bad) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -415,7 +445,8 @@ join_kernel(JoinParams P) {
     uint16_t* perm = reinterpret_cast<uint16_t*>(slice + 14 * kPool);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(slice + 16 * kPool);
     int* n_ptr = reinterpret_cast<int*>(slice + P.warp_smem_bytes - 16);
-    int2* res_pending = reinterpret_cast<int2*>(slice + P.warp_smem_bytes - 16 - 8 * 32);
+    uint16_t* long_runs = reinterpret_cast<uint16_t*>(slice + P.warp_smem_bytes - 16 - 8 * 32 -
+                                                      2 * kLongRuns);
     Pool pool;
     {
         const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
@@ -463,77 +494,91 @@ join_kernel(JoinParams P) {
             const int range_hi = min(range_lo + width, tn);
             const int rw = range_hi - range_lo;
             // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
-            for (int w = lane; w < rw / 2 + 1; w += 32) cnt[w] = 0u;
+            for (int w = 4 * lane; w < rw / 2 + 2; w += 128)
+                *reinterpret_cast<uint4*>(cnt + w) = make_uint4(0u, 0u, 0u, 0u);
             if (lane == 0) *n_ptr = 0;
             __syncwarp();
+            // the next chunk's peaks are loaded while this chunk is swept
+            float nx_mz = 0.f;
+            double nx_w = 0.0;
+            if (lane < na) {
+                nx_mz = P.A.mz[a0 + lane];
+                nx_w = __dmul_rn(peak_a(P.A.a, a0 + lane), P.A.b[a0 + lane]);
+            }
             for (int pc = 0; pc < na; pc += 32) {
                 const int p = pc + lane;
+                const float mzA = nx_mz;
+                const double wA = nx_w;
+                if (p + 32 < na) {
+                    nx_mz = P.A.mz[a0 + p + 32];
+                    nx_w = __dmul_rn(peak_a(P.A.a, a0 + p + 32), P.A.b[a0 + p + 32]);
+                }
                 if (p < na) {
-                    const double mzA = (double)P.A.mz[a0 + p];
-                    double lo_a = 0.0, hi_a = 0.0, mz2_a = 0.0, slo, shi;
-                    if (A_IS_REF) {
-                        lo_a = __dsub_rn(mzA, P.tol);
-                        hi_a = __dadd_rn(mzA, P.tol);
-                        slo = __dsub_rn(lo_a, P.shift);
-                        shi = __dsub_rn(hi_a, P.shift);
-                    } else {
-                        mz2_a = __dadd_rn(mzA, P.shift);
-                        slo = __dsub_rn(mz2_a, P.tol);
-                        shi = __dadd_rn(mz2_a, P.tol);
+                    float L, H;
+                    if (!Window<A_IS_REF, NOSHIFT>::bounds(mzA, P.tol, P.shift, L, H)) {
+                        atomicOr(P.err, kErrBadOffsets);
+                        L = 1.0f;
+                        H = 0.0f;
                     }
-                    const long long blo = bucket_of(slo, P.g.inv_w) - P.widen;
-                    const long long bhi = bucket_of(shi, P.g.inv_w) + P.widen;
-                    // the buckets of the window are one contiguous run of the
-                    // tile stream, or two when the hashed range wraps
-                    uint32_t r0b, r0e, r1b = 0, r1e = 0;
-                    if (bhi - blo + 1 >= P.g.nb) {
-                        r0b = __ldg(&T[0]);
-                        r0e = __ldg(&T[P.g.nb]);
-                    } else {
-                        const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
-                        if (bl <= bh) {
-                            r0b = __ldg(&T[bl]);
-                            r0e = __ldg(&T[bh + 1]);
-                        } else {
-                            r0b = __ldg(&T[bl]);
+                    // the window's buckets are one contiguous run of the tile
+                    // stream, or two when the hashed range wraps around
+                    uint32_t r0b = 0, r0e = 0, r1b = 0, r1e = 0;
+                    if (L <= H) {
+                        const long long blo = bucket_of(L, P.g.inv_w);
+                        const long long bhi = bucket_of(H, P.g.inv_w);
+                        if (bhi - blo + 1 >= P.g.nb) {
+                            r0b = __ldg(&T[0]);
                             r0e = __ldg(&T[P.g.nb]);
-                            r1b = __ldg(&T[0]);
-                            r1e = __ldg(&T[bh + 1]);
+                        } else {
+                            const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
+                            r0b = __ldg(&T[bl]);
+                            if (bl <= bh) {
+                                r0e = __ldg(&T[bh + 1]);
+                            } else {
+                                r0e = __ldg(&T[P.g.nb]);
+                                r1b = __ldg(&T[0]);
+                                r1e = __ldg(&T[bh + 1]);
+                            }
                         }
                     }
-                    double wA = -1.0;  // a*b of this A peak, loaded on first candidate
-                    for (int part = 0; part < 2; ++part) {
-                        const uint32_t eb = part ? r1b : r0b, ee = part ? r1e : r0e;
-                        for (uint32_t e = eb; e < ee; ++e) {
-                            const Entry en = ent[tbase + e];
-                            const int bq = (int)(en.id >> 16);
-                            if (bq < range_lo || bq >= range_hi) continue;
-                            const double mzB = (double)en.mz;
-                            bool match;
-                            if (A_IS_REF) {
-                                const double mz2 = __dadd_rn(mzB, P.shift);
-                                match = !(mz2 > hi_a) && !(mz2 < lo_a);
-                            } else {
-                                const double lo_b = __dsub_rn(mzB, P.tol);
-                                const double hi_b = __dadd_rn(mzB, P.tol);
-                                match = !(mz2_a > hi_b) && !(mz2_a < lo_b);
-                            }
-                            if (!match) continue;
-                            const int pB = (int)(en.id & 0xFFFFu);
-                            const double aB =
-                                P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
-                            if (wA < 0.0) wA = __dmul_rn(peak_a(P.A.a, a0 + p), P.A.b[a0 + p]);
+                    uint32_t e = r0b, ee = r0e;
+                    for (;;) {
+                        if (e >= ee) {
+                            if (r1e == 0) break;
+                            e = r1b;
+                            ee = r1e;
+                            r1e = 0;
+                            continue;
+                        }
+                        // up to four entries per round trip
+                        Entry en[4];
+                        const int cntE = (int)min(4u, ee - e);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (u < cntE) en[u] = ent[tbase + e + u];
+                        e += cntE;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (u >= cntE) break;
+                            const int bq = (int)(en[u].id >> 16);
+                            if (!(en[u].mz >= L) || !(en[u].mz <= H) || bq < range_lo ||
+                                bq >= range_hi)
+                                continue;
+                            const int pB = (int)(en[u].id & 0xFFFFu);
+                            const double aB = P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
                             double key;
                             uint32_t gen;
                             if (A_IS_REF) {
-                                key = __dmul_rn(__dmul_rn(wA, aB), en.b);
+                                key = __dmul_rn(__dmul_rn(wA, aB), en[u].b);
                                 gen = ((uint32_t)p << 16) | (uint32_t)pB;
                             } else {
-                                const double wB = __dmul_rn(aB, en.b);
+                                const double wB = __dmul_rn(aB, en[u].b);
                                 key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + p)),
                                                 P.A.b[a0 + p]);
                                 gen = ((uint32_t)pB << 16) | (uint32_t)p;
                             }
+                            // one pool reservation per group of lanes that found a
+                            // candidate together
                             const int slot = atomicAdd(n_ptr, 1);
                             if (slot < kPoolMax) {
                                 const int qr = bq - range_lo;
@@ -579,13 +624,14 @@ join_kernel(JoinParams P) {
             if (n > 0) {
                 // ---- counting sort of the pool by query ----
                 // exclusive scan of the per-query counts, in place (words of two)
-                const int nw = rw / 2 + 1;
-                const int per = (nw + 31) / 32;
+                const int nw = (rw / 2 + 1 + 3) & ~3;  // whole uint4s (zeroed beyond)
+                const int per = ((nw / 4 + 31) / 32) * 4;
                 const int w0 = min(nw, lane * per), w1 = min(nw, w0 + per);
                 unsigned local = 0;
-                for (int w = w0; w < w1; ++w) {
-                    const uint32_t v = cnt[w];
-                    local += (v & 0xFFFFu) + (v >> 16);
+                for (int w = w0; w < w1; w += 4) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(cnt + w);
+                    local += (v.x & 0xFFFFu) + (v.x >> 16) + (v.y & 0xFFFFu) + (v.y >> 16) +
+                             (v.z & 0xFFFFu) + (v.z >> 16) + (v.w & 0xFFFFu) + (v.w >> 16);
                 }
                 unsigned incl = local;
 #pragma unroll
@@ -611,7 +657,66 @@ join_kernel(JoinParams P) {
             // where the query index changes.  The result of a run is packed
             // into the ckey slot of its first candidate: (score f32 bits,
             // matches), matches = -1 for a pair sent to the pair kernel.
-            int n_runs = 0;
+            int n_long = 0;
+            // long runs: warp bitonic sort of (key, gen) descending in
+            // registers, then greedy by ballot (leaders in sorted order)
+            auto flush_long = [&]() {
+            for (int r = 0; r < n_long; ++r) {
+                const int i0 = long_runs[r];
+                const int q0 = pool.cq(pool.perm(i0));
+                const int L = (int)cnt_get(cnt, q0) - i0;
+                double k = -INFINITY;
+                uint32_t g = 0;
+                if (lane < L) {
+                    const int sl = pool.perm(i0 + lane);
+                    k = pool.key(sl);
+                    g = pool.gen(sl);
+                }
+#pragma unroll
+                for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+                    for (int j = kk >> 1; j > 0; j >>= 1) {
+                        const double ok = __shfl_xor_sync(full, k, j);
+                        const uint32_t og = __shfl_xor_sync(full, g, j);
+                        const bool lower = (lane & j) == 0;
+                        const bool desc = (lane & kk) == 0;
+                        // the lower lane of a descending pair keeps the larger
+                        const bool mine_first = before(k, g, ok, og);
+                        const bool keep = (lower == desc) ? mine_first : !mine_first;
+                        if (!keep) {
+                            k = ok;
+                            g = og;
+                        }
+                    }
+                }
+                bool alive = lane < L;
+                unsigned bal = __ballot_sync(full, alive);
+                double score = 0.0;
+                int mt = 0;
+                while (bal) {
+                    const int leader = __ffs(bal) - 1;
+                    const uint32_t lg = __shfl_sync(full, g, leader);
+                    const double lk = __shfl_sync(full, k, leader);
+                    score = __dadd_rn(score, lk);
+                    ++mt;
+                    if (lane == leader ||
+                        ((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu)))
+                        alive = false;
+                    bal = __ballot_sync(full, alive);
+                }
+                if (lane == 0) {
+                    const double snB = P.snB[b_begin + range_lo + q0];
+                    const float sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
+                                                                      : __dmul_rn(snB, snA));
+                    pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                }
+                __syncwarp();
+            }
+            n_long = 0;
+            };
+            // Runs of length 1 and 2 are resolved by their lane in closed
+            // form; longer runs (up to 32) are queued and resolved one at a
+            // time by the whole warp.
             for (int c = 0; c < n; c += 32) {
                 const int i = c + lane;
                 bool st = false;
@@ -620,42 +725,52 @@ join_kernel(JoinParams P) {
                     q_i = pool.cq(pool.perm(i));
                     st = (i == 0) || (pool.cq(pool.perm(i - 1)) != q_i);
                 }
-                const unsigned bal = __ballot_sync(full, st);
-                n_runs += __popc(bal);
-                // lanes starting a run resolve it now (the run ends at the next
-                // query's end counter)
-                if (st) {
-                    const int e = (int)cnt_get(cnt, q_i);
-                    const int L = e - i;
+                int L = 0;
+                if (st) L = (int)cnt_get(cnt, q_i) - i;
+                const bool is_long = st && L > 2 && L <= kLongRun && L < P.match_limit;
+                const unsigned lb = __ballot_sync(full, is_long);
+                if (n_long + __popc(lb) > kLongRuns) flush_long();
+                if (is_long) long_runs[n_long + __popc(lb & ((1u << lane) - 1u))] = (uint16_t)i;
+                n_long += __popc(lb);
+                if (st && !is_long) {
                     const int bq = b_begin + range_lo + q_i;
                     float sc;
                     int mt;
-                    if (L >= P.match_limit || L > kSmallRun) {
+                    if (L >= P.match_limit || L > kLongRun) {
                         spill_push(P.spill, A_IS_REF ? a : bq, A_IS_REF ? bq : a, P.err);
                         sc = __int_as_float(0x7fc00000);
                         mt = -1;
                     } else {
-                        double score;
-                        if (L == 1) {
-                            score = pool.key(pool.perm(i));
-                            mt = 1;
-                        } else {
-                            resolve_run(pool, i, e, score, mt);
-                        }
                         const double snB = P.snB[bq];
+                        const int s0 = pool.perm(i);
+                        double score = pool.key(s0);
+                        mt = 1;
+                        if (L == 2) {
+                            const int s1 = pool.perm(i + 1);
+                            double k0 = score, k1 = pool.key(s1);
+                            uint32_t g0 = pool.gen(s0), g1 = pool.gen(s1);
+                            if (before(k1, g1, k0, g0)) {
+                                const double tk = k0;
+                                k0 = k1;
+                                k1 = tk;
+                                const uint32_t tg = g0;
+                                g0 = g1;
+                                g1 = tg;
+                            }
+                            score = k0;
+                            if ((g0 >> 16) != (g1 >> 16) && (g0 & 0xFFFFu) != (g1 & 0xFFFFu)) {
+                                score = __dadd_rn(score, k1);
+                                mt = 2;
+                            }
+                        }
                         sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
                                                               : __dmul_rn(snB, snA));
                     }
-                    // lanes of other runs may still be reading their own slots
-                    // only; this slot belongs to this run
-                    res_pending[lane] = make_int2(__float_as_int(sc), mt);
+                    pool.set_result(pool.perm(i), make_int2(__float_as_int(sc), mt));
                 }
-                __syncwarp();
-                if (st) pool.set_result(pool.perm(i), res_pending[lane]);
-                __syncwarp();
             }
-            (void)n_runs;
-
+            __syncwarp();
+            flush_long();
             // ---- write the results ----
             if (!SPARSE) {
                 // dense row segment out[a, b_begin + range_lo ...): every query
@@ -679,12 +794,28 @@ join_kernel(JoinParams P) {
                 if ((row & 3) == 0 && (P.dense.ld & 3) == 0) {
                     for (; qv + 128 <= rw; qv += 128) {
                         const int q0 = qv + 4 * lane;
-                        float4 s4;
-                        int4 m4;
-                        result_of(q0 + 0, s4.x, m4.x);
-                        result_of(q0 + 1, s4.y, m4.y);
-                        result_of(q0 + 2, s4.z, m4.z);
-                        result_of(q0 + 3, s4.w, m4.w);
+                        float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        int4 m4 = make_int4(0, 0, 0, 0);
+                        if (n > 0) {
+                            // ends of queries q0..q0+3 and of q0-1 (= start of q0)
+                            const uint2 w = *reinterpret_cast<const uint2*>(cnt + (q0 >> 1));
+                            const unsigned e0 = w.x & 0xFFFFu, e1 = w.x >> 16;
+                            const unsigned e2 = w.y & 0xFFFFu, e3 = w.y >> 16;
+                            const unsigned sp = q0 > 0 ? (cnt[(q0 >> 1) - 1] >> 16) : 0u;
+                            if (e3 > sp) {
+                                auto fetch = [&](unsigned st, unsigned en, float& sc, int& mt) {
+                                    if (en > st) {
+                                        const int2 r = pool.result(pool.perm((int)st));
+                                        sc = __int_as_float(r.x);
+                                        mt = r.y;
+                                    }
+                                };
+                                fetch(sp, e0, s4.x, m4.x);
+                                fetch(e0, e1, s4.y, m4.y);
+                                fetch(e1, e2, s4.z, m4.z);
+                                fetch(e2, e3, s4.w, m4.w);
+                            }
+                        }
                         __stcs(reinterpret_cast<float4*>(P.dense.score + row + q0), s4);
                         __stcs(reinterpret_cast<int4*>(P.dense.matches + row + q0), m4);
                         __stcs(reinterpret_cast<uchar4*>(P.dense.overflow + row + q0),
@@ -1025,6 +1156,23 @@ void set_func_smem(T* f, size_t bytes) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
+int launch_join(cms_ctx* ctx, const JoinParams& jp, size_t smem, size_t gpool_warps,
+                cudaStream_t s) {
+    auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT>;
+    set_func_smem(kern, smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
+    const int grid = ctx->sm_count * std::max(1, per_sm);
+    if ((size_t)grid * kJoinWarps > gpool_warps) {
+        set_error("cms_cosine_greedy: join grid larger than its scratch");
+        return CMS_ERR_CUDA;
+    }
+    kern<<<grid, kJoinThreads, smem, s>>>(jp);
+    CMS_CUDA_TRY(cudaGetLastError());
+    return CMS_OK;
+}
+
 int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
                const SparseOut* sparse, const cms_cosine_config* cfg, cudaStream_t s) {
     Plan p;
@@ -1163,7 +1311,6 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.tol = args.tol;
     jp.shift = args.shift;
     jp.match_limit = args.match_limit;
-    jp.widen = args.shift != 0.0 ? 1 : 0;
     jp.init_width_scale = 0.f;
     if (cfg && cfg->cand_per_pair > 0.0 && args.ref.n > 0) {
         // expected candidates of (A spectrum with n peaks, w queries) ~ n*w*lambda
@@ -1172,6 +1319,7 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
     }
     jp.warp_smem_bytes = warp_slice_bytes(p.tile);
+    jp.gpool = gpool;
     jp.work = work_join;
     jp.spill = SpillList{spill, spill_count, p.spill_cap};
     jp.dense = pp.dense;
@@ -1179,28 +1327,14 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.err = ctx->err_word;
     jp.bad = bad;
     const size_t join_smem = (size_t)warp_slice_bytes(p.tile) * kJoinWarps;
-    int join_blocks_per_sm = 1;
     {
-    StageScope sc(ctx, 3, 1, s);
-    if (sparse) {
-        set_func_smem(join_kernel<true, true>, join_smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, true>,
-                                                      kJoinThreads, join_smem);
-    } else {
-        set_func_smem(join_kernel<true, false>, join_smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&join_blocks_per_sm, join_kernel<true, false>,
-                                                      kJoinThreads, join_smem);
-    }
-    const int join_grid = ctx->sm_count * std::max(1, join_blocks_per_sm);
-    jp.gpool = gpool;
-    if ((size_t)join_grid * kJoinWarps > gpool_warps) {
-        set_error("cms_cosine_greedy: join grid larger than its scratch");
-        return CMS_ERR_CUDA;
-    }
-    if (sparse)
-        join_kernel<true, true><<<join_grid, kJoinThreads, join_smem, s>>>(jp);
-    else
-        join_kernel<true, false><<<join_grid, kJoinThreads, join_smem, s>>>(jp);
+        StageScope sc(ctx, 3, 1, s);
+        const bool noshift = args.shift == 0.0;
+        rc = sparse ? (noshift ? launch_join<true, true, true>(ctx, jp, join_smem, gpool_warps, s)
+                               : launch_join<true, true, false>(ctx, jp, join_smem, gpool_warps, s))
+                    : (noshift ? launch_join<true, false, true>(ctx, jp, join_smem, gpool_warps, s)
+                               : launch_join<true, false, false>(ctx, jp, join_smem, gpool_warps, s));
+        if (rc) return rc;
     }
     CMS_CUDA_TRY(cudaGetLastError());
 

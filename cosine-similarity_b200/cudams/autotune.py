@@ -74,7 +74,8 @@ def heuristic_config(stats: WorkloadStats, n_q: int) -> dict:
     if stats.cand_per_pair >= DENSE_CANDIDATES:
         return {"mode": 2}
     per_pair = max(stats.cand_per_pair, 1e-4)
-    tile = int(0.4 * POOL / per_pair)
+    # measured optimum on B200: ~70 expected candidates per (reference, tile)
+    tile = int(70.0 / per_pair)
     tile = max(32, min(4096, tile))
     tile = (tile + 31) // 32 * 32
     tile = min(tile, max(32, (n_q + 31) // 32 * 32))
