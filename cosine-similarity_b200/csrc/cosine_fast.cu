@@ -36,6 +36,7 @@
 //                        used-peak bitmasks.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "cms_internal.cuh"
 
@@ -1431,4 +1432,148 @@ extern "C" int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const
     SparseOut out{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
                   reinterpret_cast<unsigned long long*>(hit_count), threshold};
     return run_cosine(ctx, args, nullptr, &out, cfg, s);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant (cms_cosine_greedy_noalloc)
+//
+// Some callers cannot let a library call cudaMalloc: an application whose
+// device memory is already reserved by its own allocator (a framework's
+// caching pool that owns almost all of the GPU), a latency-critical loop that
+// cannot afford the device-wide synchronisation cudaMalloc/cudaFree may
+// imply, or a plugin host that forbids libraries to allocate behind its back.
+// For them this entry point runs the dense greedy cosine with the pair kernel
+// over every pair, and keeps its only scratch -- validity flags and the two
+// per-spectrum norm arrays -- in the fixed device array below instead of a
+// context's arena.  The array is part of the library's device image: every
+// GPU that loads the library holds it until the process exits.
+// ---------------------------------------------------------------------------
+namespace cms {
+namespace {
+
+constexpr int64_t kNoAllocMaxSpectra = int64_t(1) << 20;  // n_ref + n_q
+constexpr size_t kNoAllocHeader = 256;                     // flags and error word
+constexpr size_t kNoAllocBytes = kNoAllocHeader + 8 * (size_t)kNoAllocMaxSpectra + 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device, with that device current, and cached.
+int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    CMS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("cms_cosine_greedy_noalloc: device ordinal %d out of range", dev);
+        return CMS_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CMS_OK;
+}
+
+}  // namespace
+}  // namespace cms
+
+extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a,
+                                         const double* ref_b, const int64_t* ref_off,
+                                         int64_t n_ref, int64_t n_ref_peaks, const float* q_mz,
+                                         const double* q_a, const double* q_b,
+                                         const int64_t* q_off, int64_t n_q, int64_t n_q_peaks,
+                                         double tolerance, double shift, int match_limit,
+                                         float* score, int32_t* matches, uint8_t* overflow,
+                                         int64_t ld, uint32_t* device_error, void* stream) {
+    using namespace cms;
+    CosineArgs args{SpecSet{ref_mz, ref_a, ref_b, ref_off, n_ref, n_ref_peaks},
+                    SpecSet{q_mz, q_a, q_b, q_off, n_q, n_q_peaks}, tolerance, shift,
+                    match_limit};
+    if (!check_common(args, "cms_cosine_greedy_noalloc")) return CMS_ERR_INVALID;
+    if (ld < n_q) {
+        set_error("cms_cosine_greedy_noalloc: ld < n_q");
+        return CMS_ERR_INVALID;
+    }
+    if (n_ref + n_q > kNoAllocMaxSpectra) {
+        set_error("cms_cosine_greedy_noalloc: n_ref + n_q = %lld exceeds the fixed scratch "
+                  "capacity of %lld spectra; split the call or use cms_cosine_greedy",
+                  (long long)(n_ref + n_q), (long long)kNoAllocMaxSpectra);
+        return CMS_ERR_UNSUPPORTED;
+    }
+    if (match_limit > 4096) {
+        set_error("cms_cosine_greedy_noalloc: match_limit must be <= 4096");
+        return CMS_ERR_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_ref == 0 || n_q == 0) {
+        if (device_error) CMS_CUDA_TRY(cudaMemsetAsync(device_error, 0, sizeof(uint32_t), s));
+        return CMS_OK;
+    }
+    if (!score || !matches || !overflow) {
+        set_error("cms_cosine_greedy_noalloc: null output pointer");
+        return CMS_ERR_INVALID;
+    }
+    unsigned char* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    uint32_t* bad = reinterpret_cast<uint32_t*>(base);
+    uint32_t* err = reinterpret_cast<uint32_t*>(base + 4);
+    double* snR = reinterpret_cast<double*>(base + kNoAllocHeader);
+    double* snQ = snR + n_ref;
+    // the array keeps the previous call's contents: reset the flags
+    CMS_CUDA_TRY(cudaMemsetAsync(base, 0, kNoAllocHeader, s));
+
+    int dev = 0, sms = 0;
+    CMS_CUDA_TRY(cudaGetDevice(&dev));
+    CMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int threads = 256;
+    auto grid_for = [&](int64_t n) {
+        return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads,
+                                                           (int64_t)sms * 32));
+    };
+    validate_kernel<<<grid_for(n_ref), threads, 0, s>>>(args.ref, bad, err);
+    validate_kernel<<<grid_for(n_q), threads, 0, s>>>(args.qry, bad, err);
+    norms_kernel<<<grid_for(n_ref), threads, 0, s>>>(args.ref, snR, bad);
+    norms_kernel<<<grid_for(n_q), threads, 0, s>>>(args.qry, snQ, bad);
+    CMS_CUDA_TRY(cudaGetLastError());
+
+    PairParams pp;
+    pp.R = args.ref;
+    pp.Q = args.qry;
+    pp.snR = snR;
+    pp.snQ = snQ;
+    pp.tol = tolerance;
+    pp.shift = shift;
+    pp.match_limit = match_limit;
+    int cap = 2;
+    while (cap < match_limit) cap <<= 1;
+    pp.cap = cap;
+    pp.pairs = nullptr;  // every pair of R x Q, statically strided
+    pp.n_pairs = nullptr;
+    pp.pairs_cap = 0;
+    pp.work = reinterpret_cast<unsigned long long*>(base + 8);
+    pp.dense = DenseOut{score, matches, overflow, ld};
+    pp.sparse = SparseOut{};
+    pp.err = err;
+    pp.bad = bad;
+    const int pair_threads = 128;
+    const size_t pair_smem = (size_t)cap * 12 + 2 * 2048 * 4;
+    CMS_CUDA_TRY(cudaFuncSetAttribute(pair_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)pair_smem));
+    int per_sm = 1;
+    CMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<false>,
+                                                               pair_threads, pair_smem));
+    pair_kernel<false><<<sms * std::max(1, per_sm), pair_threads, pair_smem, s>>>(pp);
+    CMS_CUDA_TRY(cudaGetLastError());
+    if (device_error)
+        CMS_CUDA_TRY(cudaMemcpyAsync(device_error, err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    return CMS_OK;
 }

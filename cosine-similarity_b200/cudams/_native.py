@@ -54,6 +54,11 @@ SIGNATURES = {
         _p, _p, _p, _p, c_int64, c_int64,
         c_double, c_double, c_int, c_float,
         _p, _p, _p, _p, _p, c_int64, _p, _p, _p]),
+    "cms_cosine_greedy_noalloc": (c_int, [
+        _p, _p, _p, _p, c_int64, c_int64,
+        _p, _p, _p, _p, c_int64, c_int64,
+        c_double, c_double, c_int,
+        _p, _p, _p, c_int64, _p, _p]),
     "cms_profile_enable": (c_int, [_p, c_int]),
     "cms_profile_read": (c_int, [_p, _p, _p, c_int]),
     "cms_fingerprint": (c_int, [

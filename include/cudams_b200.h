@@ -178,6 +178,39 @@ int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* re
                              void* stream);
 
 /*
+ * Allocation-free greedy cosine, dense output.  No counterpart in the
+ * reference: this entry point exists for callers that must not have a
+ * library allocate device memory -- an application whose GPU memory is
+ * already reserved by its own allocator, a latency-critical loop that cannot
+ * take the device-wide synchronisation cudaMalloc / cudaFree may imply, or a
+ * plugin host that forbids allocations behind its back.  It needs no context,
+ * calls no cudaMalloc, cudaFree or other allocating routine, and computes the
+ * same results as cms_cosine_greedy (same arguments and numerics) with the
+ * pair kernel over every pair, which is exact for any input but slower than
+ * the indexed join when most pairs have no candidates.
+ *   - Scratch: a fixed device array of the library, about 8 MiB (flags plus
+ *     one float64 norm per spectrum); every GPU that loads the library holds
+ *     it until the process exits.  Limit: n_ref + n_q <= 1048576 spectra and
+ *     match_limit <= 4096; larger calls fail with CMS_ERR_UNSUPPORTED.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress) and caches it; make that first call before any
+ *     stream capture begins.
+ *   - All calls share the one array, and it keeps the last call's contents
+ *     (the call clears the flags it needs): calls that overlap on the GPU,
+ *     from different streams or host threads, race and corrupt each other.
+ *     Serialise them.
+ *   - device_error (device uint32, may be NULL) receives the error bits of
+ *     this call (see cms_take_device_error); 0 means the results are valid.
+ */
+int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a, const double* ref_b,
+                              const int64_t* ref_off, int64_t n_ref, int64_t n_ref_peaks,
+                              const float* q_mz, const double* q_a, const double* q_b,
+                              const int64_t* q_off, int64_t n_q, int64_t n_q_peaks,
+                              double tolerance, double shift, int match_limit, float* score,
+                              int32_t* matches, uint8_t* overflow, int64_t ld,
+                              uint32_t* device_error, void* stream);
+
+/*
  * Fingerprint similarity on bit-packed fingerprints: n_words uint32 per
  * row, bit k in word k/32 at bit k%32, unused high bits zero.  Writes
  * out[i*ld + j] (float32) for every (reference i, query j):
