@@ -50,6 +50,10 @@ TOL, MATCH_LIMIT, N_MAX_PEAKS = 0.01, 4096, 1024
 WORKLOAD = ("batched greedy cosine 100k x 100k, lognormal peaks (median 60, sigma 1.0, "
             "clip 5-1000), m/z U(50,2000), tol 0.01, powers (0,1), match_limit 4096")
 BYTES_PER_PAIR = 9
+# DRAM bytes per pair of join_kernel (read + write), from an ncu capture of the
+# 20k x 20k case of this workload (profiles/join_kernel_batched_cosine_20k.txt);
+# traffic grows with pairs, so a full launch is scaled by its pair count.
+JOIN_TRAFFIC_BYTES_PER_PAIR = 10.35
 
 
 def parse():
@@ -58,7 +62,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=100_000, help="spectra per side (default 100k)")
+    ap.add_argument("--spectra", dest="n", type=int, default=100_000, help="spectra per side (default 100k)")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--plain-rows", type=int, default=0, help="rows for the plain sample (0=auto)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -66,6 +70,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--config", type=str, default="", help="JSON cms_cosine_config override")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other workloads")
     return ap.parse_args()
 
 
@@ -311,7 +316,9 @@ def run_ours(args, world, rank, local):
     hbm, peak_kind = measured_peaks()
     achieved = alg_bytes / (join_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": "join_kernel", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": JOIN_TRAFFIC_BYTES_PER_PAIR * pairs_per_launch,
+                "traffic_source": "ncu dram bytes of a 20k x 20k capture, scaled by pairs",
                 "peak_source": f"{peak_kind} hbm_gbs (copy)",
                 "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": join_ms,
                 "stage_ms_per_step": {n: float(v) / args.steps for n, v in zip(names, stage_ms)},
@@ -370,8 +377,113 @@ def run_ours(args, world, rank, local):
 
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ref, qry, args.cpu_seconds)
+    del out, sub, rd, qd
+    ref._device.clear()
+    qry._device.clear()
+    torch.cuda.empty_cache()
+    if rank == 0 and not args.no_extra:
+        line["other_workloads"] = other_workloads(dev, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _time_ms(fn, reps=3):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def other_workloads(dev, args):
+    """The other workloads, each bounded to seconds: device-resident pairs/s."""
+    import numpy as np
+    import torch
+
+    from cudams import autotune, kernels, synthetic
+
+    res = {}
+    # fingerprint similarity, 100k x 100k 2048-bit, jaccard/dice/cosine
+    n_fp = min(args.n, 100_000)
+    bits = synthetic.fingerprints(2 * n_fp, seed=args.seed)
+    rb = torch.from_numpy(bits[:n_fp]).to(dev)
+    qb = torch.from_numpy(bits[n_fp:]).to(dev)
+    fout = torch.empty((n_fp, n_fp), dtype=torch.float32, device=dev)
+    fp = {}
+    for m in ("jaccard", "dice", "cosine"):
+        ms = _time_ms(lambda: kernels.fingerprint_matrix(m, rb, None, qb, None, 64, float("nan"),
+                                                         out=fout))
+        fp[m] = n_fp * n_fp / (ms / 1e3)
+    del fout
+    torch.cuda.empty_cache()
+    # the reference's own torch formulation (float32 GEMM + elementwise) on a 20k tile
+    nt = min(20_000, n_fp)
+    R = torch.from_numpy(np.unpackbits(bits[:nt].view(np.uint8), axis=1,
+                                       bitorder="little")).to(dev).float()
+    Q = torch.from_numpy(np.unpackbits(bits[n_fp:n_fp + nt].view(np.uint8), axis=1,
+                                       bitorder="little")).to(dev).float()
+
+    def torch_jaccard():
+        inter = R @ Q.T
+        u = R.sum(1, keepdim=True) + Q.sum(1, keepdim=True).T
+        u -= inter
+        return inter.div(u).nan_to_num()
+
+    tms = _time_ms(torch_jaccard)
+    del R, Q
+    torch.cuda.empty_cache()
+    popc_peak = 148 * 16 * 1965e6 / 2  # 64-bit popcounts/s at 16 POPC32 per clock per SM
+    res["fingerprint_100k"] = {
+        "workload": f"{n_fp} x {n_fp} fingerprints, 2048 bits, density U(5%,15%)",
+        "pairs_per_s": fp, "unit": "pairs/s",
+        "roofline": {"bound": "int-pipe popcount", "achieved_popc64_per_s": 32 * fp["jaccard"],
+                     "peak_popc64_per_s": popc_peak, "frac": 32 * fp["jaccard"] / popc_peak,
+                     "hbm_frac": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
+        "reference_torch_cuda_jaccard_pairs_per_s": nt * nt / (tms / 1e3),
+        "reference_torch_sample": f"{nt} x {nt}"}
+
+    # 1024 x 1024 uniform spectra, tol 0.1 (the reference's CPU-runnable case)
+    u_r = synthetic.uniform_spectra(1024, seed=args.seed + 1).to_device(dev)
+    u_q = synthetic.uniform_spectra(1024, seed=args.seed + 2).to_device(dev)
+    u_cfg = autotune.choose_config(synthetic.uniform_spectra(1024, seed=args.seed + 1),
+                                   synthetic.uniform_spectra(1024, seed=args.seed + 2), 0.1)
+    ms_t = _time_ms(lambda: kernels.cosine_greedy_dense(u_r, u_q, 0.1, 0.0, 2048, config=u_cfg))
+    ms_p = _time_ms(lambda: kernels.cosine_greedy_plain(u_r, u_q, 0.1, 0.0, 2048, 1024))
+    res["uniform_1k"] = {"workload": "1024 x 1024, peaks U{10..200}, tol 0.1, match_limit 2048",
+                         "tiled_pairs_per_s": 1024 * 1024 / (ms_t / 1e3),
+                         "plain_pairs_per_s": 1024 * 1024 / (ms_p / 1e3), "tiled_ms": ms_t,
+                         "tuning": u_cfg}
+
+    # overflow stress: clustered dense spectra, 20k x 20k, nearly every pair overflows
+    c_r = synthetic.clustered_spectra(20_000, seed=args.seed + 3)
+    c_q = synthetic.clustered_spectra(20_000, seed=args.seed + 4)
+    cfg = autotune.choose_config(c_r, c_q, 0.05)
+    rows = 1000
+    cr_sub = c_r.subset(0, rows).to_device(dev)
+    cq = c_q.to_device(dev)
+    cout = tuple(torch.empty((rows, c_q.n), dtype=t, device=dev)
+                 for t in (torch.float32, torch.int32, torch.uint8))
+    ms_o = _time_ms(lambda: kernels.cosine_greedy_dense(cr_sub, cq, 0.05, 0.0, 1024, out=cout,
+                                                         config=cfg), reps=1)
+    ovf = float(cout[2].float().mean().item())
+    prow = 64
+    cr_p = c_r.subset(0, prow).to_device(dev)
+    pout = tuple(t[:prow] for t in cout)
+    ms_pl = _time_ms(lambda: kernels.cosine_greedy_plain(cr_p, cq, 0.05, 0.0, 1024, 2048,
+                                                          out=pout), reps=1)
+    res["overflow_stress_20k"] = {
+        "workload": "20k x 20k clustered (200 centres, sigma 0.02), 1000-2000 peaks, tol 0.05, "
+                    "powers (3, 0.6), match_limit 1024",
+        "tiled_pairs_per_s": rows * c_q.n / (ms_o / 1e3), "tiled_sample": f"{rows} x {c_q.n}",
+        "plain_pairs_per_s": prow * c_q.n / (ms_pl / 1e3), "plain_sample": f"{prow} x {c_q.n}",
+        "overflow_fraction": ovf, "tuning": cfg}
+    return res
 
 
 def main():

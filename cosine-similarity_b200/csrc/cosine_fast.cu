@@ -1122,7 +1122,14 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
         set_error("cms_cosine_greedy: mode must be 0, 1 or 2");
         return CMS_ERR_INVALID;
     }
-    p.tile = (cfg && cfg->tile_spectra > 0) ? cfg->tile_spectra : 1024;
+    if (cfg && cfg->tile_spectra > 0) {
+        p.tile = cfg->tile_spectra;
+    } else {
+        // enough work items (reference x tile) to fill every resident warp
+        // several times over, at most 1024 queries per tile
+        const long long pairs = (long long)args.ref.n * (long long)args.qry.n;
+        p.tile = (int)std::max<long long>(32, std::min<long long>(1024, pairs / 40000));
+    }
     if (p.tile > kMaxTile) {
         set_error("cms_cosine_greedy: tile_spectra must be <= %d", kMaxTile);
         return CMS_ERR_UNSUPPORTED;

@@ -70,12 +70,19 @@ def workload_stats(ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
                          float(qry.lengths.mean()) if qry.n else 0.0)
 
 
-def heuristic_config(stats: WorkloadStats, n_q: int) -> dict:
+# work items (reference spectrum x query tile) wanted per launch: several per
+# resident warp of the join kernel (148 SMs x 32 warps), so that small
+# problems still fill the GPU
+TARGET_ITEMS = 40_000
+
+
+def heuristic_config(stats: WorkloadStats, n_q: int, n_ref: int = 1 << 30) -> dict:
     if stats.cand_per_pair >= DENSE_CANDIDATES:
         return {"mode": 2}
     per_pair = max(stats.cand_per_pair, 1e-4)
     # measured optimum on B200: ~70 expected candidates per (reference, tile)
     tile = int(70.0 / per_pair)
+    tile = min(tile, max(32, (n_ref * n_q) // TARGET_ITEMS))
     tile = max(32, min(4096, tile))
     tile = (tile + 31) // 32 * 32
     tile = min(tile, max(32, (n_q + 31) // 32 * 32))
@@ -107,7 +114,7 @@ class Tuner:
                 self._cache = {}
         return self._cache
 
-    def lookup(self, stats: WorkloadStats, gpu: str, n_q: int) -> dict:
+    def lookup(self, stats: WorkloadStats, gpu: str, n_q: int, n_ref: int = 1 << 30) -> dict:
         with self._lock:
             hit = self._load().get(self.key(stats, gpu))
         if hit:
@@ -115,7 +122,7 @@ class Tuner:
             if cfg.get("tile_spectra"):
                 cfg["tile_spectra"] = min(cfg["tile_spectra"], max(32, n_q))
             return cfg
-        return heuristic_config(stats, n_q)
+        return heuristic_config(stats, n_q, n_ref)
 
     def record(self, stats: WorkloadStats, gpu: str, config: dict) -> None:
         with self._lock:
@@ -134,4 +141,4 @@ _default = Tuner()
 def choose_config(ref: PackedSpectra, qry: PackedSpectra, tolerance: float, shift: float = 0.0,
                   gpu: str = "B200") -> dict:
     stats = workload_stats(ref, qry, tolerance, shift)
-    return _default.lookup(stats, gpu, qry.n)
+    return _default.lookup(stats, gpu, qry.n, ref.n)
