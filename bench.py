@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--config", type=str, default="", help="JSON cms_cosine_config override")
     ap.add_argument("--no-extra", action="store_true", help="skip the other workloads")
+    ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     return ap.parse_args()
 
 
@@ -383,6 +384,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.empty_cache()
     if rank == 0 and not args.no_extra:
         line["other_workloads"] = other_workloads(dev, args)
+    if rank == 0 and not args.no_served:
+        line["served"] = served_workload(dev, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -484,6 +487,70 @@ def other_workloads(dev, args):
         "plain_pairs_per_s": prow * c_q.n / (ms_pl / 1e3), "plain_sample": f"{prow} x {c_q.n}",
         "overflow_fraction": ovf, "tuning": cfg}
     return res
+
+
+def served_workload(dev, args, seconds: float = 15.0, rate_1k: float = 20.0,
+                    rate_bg: float = 20.0, library_size: int = 1_000_000):
+    """Resident 1M-spectrum library, Poisson-arriving query batches: 1000-query
+    batches at rate_1k per second plus background batches of log-uniform size in
+    [1, 4096] at rate_bg per second; sparse output of scores >= 0.7."""
+    import numpy as np
+    import torch
+
+    from cudams import synthetic
+    from cudams.serving import Server, SpectrumLibrary
+
+    libp = synthetic.lognormal_spectra(library_size, seed=args.seed + 10)
+    t = time.perf_counter()
+    lib = SpectrumLibrary(libp, tolerance=TOL, match_limit=MATCH_LIMIT, n_max_peaks=N_MAX_PEAKS)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t
+    pool = synthetic.lognormal_spectra(60_000, seed=args.seed + 11)
+    rng = np.random.default_rng(args.seed + 12)
+    alone = []
+    for i in range(5):
+        alone.append(lib.search(pool.subset(1000 * i, 1000 * (i + 1)), 0.7).latency_s)
+    futs, kinds = [], []
+    try:
+        with Server(lib, threshold=0.7, slots=4) as srv:
+            t0 = time.perf_counter()
+            nxt1 = t0 + rng.exponential(1 / rate_1k)
+            nxt2 = t0 + rng.exponential(1 / rate_bg)
+            off = 0
+            while True:
+                now = time.perf_counter()
+                if now - t0 >= seconds:
+                    break
+                if now >= nxt1:
+                    futs.append(srv.submit(pool.subset(off % 59000, off % 59000 + 1000)))
+                    kinds.append(1000)
+                    off += 1000
+                    nxt1 += rng.exponential(1 / rate_1k)
+                if now >= nxt2:
+                    k = int(np.exp(rng.uniform(0.0, np.log(4096.0))))
+                    futs.append(srv.submit(pool.subset(off % 55000, off % 55000 + k)))
+                    kinds.append(k)
+                    off += k
+                    nxt2 += rng.exponential(1 / rate_bg)
+                time.sleep(max(0.0, min(nxt1, nxt2) - time.perf_counter() - 2e-4))
+            res = [f.result() for f in futs]
+            elapsed = time.perf_counter() - t0
+            concurrent = srv.max_concurrent
+    finally:
+        lib.close()
+    lat_1k = np.array([r.latency_s for r, k in zip(res, kinds) if k == 1000]) * 1e3
+    lat = np.array([r.latency_s for r in res]) * 1e3
+    return {
+        "workload": f"resident library of {library_size} lognormal spectra, tol {TOL}, "
+                    f"match_limit {MATCH_LIMIT}; Poisson arrivals: 1000-query batches at "
+                    f"{rate_1k}/s + log-uniform [1, 4096]-query batches at {rate_bg}/s for "
+                    f"{seconds:.0f} s; sparse output score >= 0.7; 4 slots",
+        "library_build_s": build_s, "requests": len(res), "requests_1k": int(lat_1k.size),
+        "p50_ms_1k": float(np.percentile(lat_1k, 50)), "p99_ms_1k": float(np.percentile(lat_1k, 99)),
+        "p50_ms_all": float(np.percentile(lat, 50)), "p99_ms_all": float(np.percentile(lat, 99)),
+        "latency_1k_alone_ms": float(1e3 * np.median(alone)),
+        "pairs_per_s": sum(r.pairs for r in res) / elapsed,
+        "max_concurrent_requests": concurrent, "hits": int(sum(r.ref.shape[0] for r in res))}
 
 
 def main():

@@ -252,6 +252,18 @@ __device__ __forceinline__ bool before(double k1, uint32_t g1, double k2, uint32
     return k1 > k2 || (k1 == k2 && g1 > g2);
 }
 
+__device__ __forceinline__ void emit_hit(const SparseOut& o, int r, int q, float sc, int mt,
+                                         uint8_t ovf) {
+    const unsigned long long pos = atomicAdd(o.count, 1ull);
+    if (pos < (unsigned long long)o.capacity) {
+        o.r[pos] = r;
+        o.q[pos] = q;
+        o.score[pos] = sc;
+        o.matches[pos] = mt;
+        o.overflow[pos] = ovf;
+    }
+}
+
 struct SpillList {
     int2* pairs;  // (reference, query)
     unsigned int* count;
@@ -706,10 +718,16 @@ join_kernel(JoinParams P) {
                     bal = __ballot_sync(full, alive);
                 }
                 if (lane == 0) {
-                    const double snB = P.snB[b_begin + range_lo + q0];
+                    const int bq = b_begin + range_lo + q0;
+                    const double snB = P.snB[bq];
                     const float sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
                                                                       : __dmul_rn(snB, snA));
-                    pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                    if (SPARSE) {
+                        if (sc >= P.sparse.threshold)
+                            emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
+                    } else {
+                        pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                    }
                 }
                 __syncwarp();
             }
@@ -767,12 +785,17 @@ join_kernel(JoinParams P) {
                         sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
                                                               : __dmul_rn(snB, snA));
                     }
-                    pool.set_result(pool.perm(i), make_int2(__float_as_int(sc), mt));
+                    if (SPARSE) {
+                        if (mt > 0 && sc >= P.sparse.threshold)
+                            emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
+                    } else {
+                        pool.set_result(pool.perm(i), make_int2(__float_as_int(sc), mt));
+                    }
                 }
             }
             __syncwarp();
             flush_long();
-            // ---- write the results ----
+            // ---- write the results (sparse hits were emitted above) ----
             if (!SPARSE) {
                 // dense row segment out[a, b_begin + range_lo ...): every query
                 // of the range, zeros where there is no candidate; 4 queries per
@@ -830,41 +853,6 @@ join_kernel(JoinParams P) {
                     __stcs(&P.dense.score[row + qr], sc);
                     __stcs(&P.dense.matches[row + qr], mt);
                     __stcs(&P.dense.overflow[row + qr], (unsigned char)0);
-                }
-            } else if (n > 0) {
-                for (int c = 0; c < rw; c += 32) {
-                    const int qr = c + lane;
-                    bool hit = false;
-                    float sc = 0.f;
-                    int mt = 0;
-                    const int bq = b_begin + range_lo + qr;
-                    if (qr < rw) {
-                        const int e = (int)cnt_get(cnt, qr);
-                        const int s = qr > 0 ? (int)cnt_get(cnt, qr - 1) : 0;
-                        if (e > s) {
-                            const int2 r = pool.result(pool.perm(s));
-                            sc = __int_as_float(r.x);
-                            mt = r.y;
-                            hit = mt >= 0 && sc >= P.sparse.threshold;
-                        }
-                    }
-                    const unsigned bal = __ballot_sync(full, hit);
-                    if (bal) {
-                        unsigned long long hb = 0;
-                        if (lane == 0)
-                            hb = atomicAdd(P.sparse.count, (unsigned long long)__popc(bal));
-                        hb = __shfl_sync(full, hb, 0);
-                        if (hit) {
-                            const unsigned long long pos = hb + __popc(bal & ((1u << lane) - 1u));
-                            if (pos < (unsigned long long)P.sparse.capacity) {
-                                P.sparse.r[pos] = A_IS_REF ? a : bq;
-                                P.sparse.q[pos] = A_IS_REF ? bq : a;
-                                P.sparse.score[pos] = sc;
-                                P.sparse.matches[pos] = mt;
-                                P.sparse.overflow[pos] = 0;
-                            }
-                        }
-                    }
                 }
             }
             __syncwarp();
@@ -1083,14 +1071,7 @@ __global__ void pair_kernel(PairParams P) {
                 P.dense.matches[o] = matches;
                 P.dense.overflow[o] = overflow ? 1 : 0;
             } else if (n > 0 && sc >= P.sparse.threshold) {
-                const unsigned long long pos = atomicAdd(P.sparse.count, 1ull);
-                if (pos < (unsigned long long)P.sparse.capacity) {
-                    P.sparse.r[pos] = (int32_t)ri;
-                    P.sparse.q[pos] = (int32_t)qi;
-                    P.sparse.score[pos] = sc;
-                    P.sparse.matches[pos] = matches;
-                    P.sparse.overflow[pos] = overflow ? 1 : 0;
-                }
+                emit_hit(P.sparse, (int)ri, (int)qi, sc, matches, overflow ? 1 : 0);
             }
         }
     }
@@ -1166,12 +1147,13 @@ void set_func_smem(T* f, size_t bytes) {
 
 template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
 int launch_join(cms_ctx* ctx, const JoinParams& jp, size_t smem, size_t gpool_warps,
-                cudaStream_t s) {
+                cudaStream_t s, int max_grid = 0) {
     auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT>;
     set_func_smem(kern, smem);
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
-    const int grid = ctx->sm_count * std::max(1, per_sm);
+    int grid = ctx->sm_count * std::max(1, per_sm);
+    if (max_grid > 0) grid = std::min(grid, max_grid);
     if ((size_t)grid * kJoinWarps > gpool_warps) {
         set_error("cms_cosine_greedy: join grid larger than its scratch");
         return CMS_ERR_CUDA;
@@ -1582,5 +1564,278 @@ extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_
     CMS_CUDA_TRY(cudaGetLastError());
     if (device_error)
         CMS_CUDA_TRY(cudaMemcpyAsync(device_error, err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    return CMS_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Resident library (cms_library_*): the indexed side built once, searched by
+// many query batches.
+// ---------------------------------------------------------------------------
+struct cms_library {
+    int device = 0;
+    cms::SpecSet spec{};  // caller-owned device arrays; must outlive the library
+    double tol = 0.0, shift = 0.0, cand_per_pair = 0.0;
+    int match_limit = 1;
+    cms::IndexGeom g{};
+    double* sn = nullptr;
+    uint32_t* tab = nullptr;
+    cms::Entry* ent = nullptr;
+    uint32_t* bad = nullptr;
+};
+
+namespace {
+void library_free(cms_library* L) {
+    if (!L) return;
+    cudaFree(L->sn);
+    cudaFree(L->tab);
+    cudaFree(L->ent);
+    cudaFree(L->bad);
+    delete L;
+}
+}  // namespace
+
+extern "C" int cms_library_create(cms_ctx* ctx, const float* mz, const double* a, const double* b,
+                                  const int64_t* off, int64_t n, int64_t n_peaks,
+                                  double tolerance, double shift, int match_limit,
+                                  const cms_cosine_config* cfg, cms_library** out, void* stream) {
+    using namespace cms;
+    if (!ctx || !out) {
+        set_error("cms_library_create: null context or output");
+        return CMS_ERR_INVALID;
+    }
+    *out = nullptr;
+    CosineArgs args{SpecSet{mz, a, b, off, n, n_peaks}, SpecSet{mz, a, b, off, n, n_peaks},
+                    tolerance, shift, match_limit};
+    if (!check_common(args, "cms_library_create")) return CMS_ERR_INVALID;
+    if (n <= 0) {
+        set_error("cms_library_create: empty library");
+        return CMS_ERR_INVALID;
+    }
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    cms_library* L = new cms_library();
+    L->device = ctx->device;
+    L->spec = args.ref;
+    L->tol = tolerance;
+    L->shift = shift;
+    L->match_limit = match_limit;
+    L->cand_per_pair = (cfg && cfg->cand_per_pair > 0.0) ? cfg->cand_per_pair : 0.0;
+    const int tile = (int)std::min<int64_t>((cfg && cfg->tile_spectra > 0) ? cfg->tile_spectra
+                                                                            : 1024, n);
+    if (tile > kMaxTile) {
+        delete L;
+        set_error("cms_library_create: tile_spectra must be <= %d", kMaxTile);
+        return CMS_ERR_UNSUPPORTED;
+    }
+    double w = (cfg && cfg->bucket_width > 0.0) ? cfg->bucket_width : 2.0 * tolerance;
+    if (w < tolerance) w = tolerance;
+    if (!(w > 0.0)) w = 1e-3;
+    const double avg_tile_peaks = (double)n_peaks * tile / (double)n;
+    int nb = (cfg && cfg->n_buckets > 0) ? next_pow2(cfg->n_buckets)
+                                         : next_pow2((long long)std::max(1024.0, avg_tile_peaks));
+    nb = std::min(nb, 1 << 22);
+    L->g = IndexGeom{tile, (int)((n + tile - 1) / tile), nb, 1.0 / w};
+    const size_t n_tab = (size_t)L->g.n_tiles * (nb + 1), n_cur = (size_t)L->g.n_tiles * nb;
+    uint32_t* cur = nullptr;
+    cudaError_t e = cudaMalloc(&L->bad, 64);
+    if (e == cudaSuccess) e = cudaMalloc(&L->sn, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&L->tab, sizeof(uint32_t) * n_tab);
+    if (e == cudaSuccess) e = cudaMalloc(&L->ent, sizeof(Entry) * std::max<int64_t>(1, n_peaks));
+    if (e == cudaSuccess) e = cudaMalloc(&cur, sizeof(uint32_t) * n_cur);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaFree(cur);
+        library_free(L);
+        set_error("cms_library_create: device allocation failed (%s)", cudaGetErrorString(e));
+        return CMS_ERR_NOMEM;
+    }
+    const int threads = 256;
+    auto grid_for = [&](int64_t cnt) {
+        return (int)std::max<int64_t>(1, std::min<int64_t>((cnt + threads - 1) / threads,
+                                                           (int64_t)ctx->sm_count * 32));
+    };
+    e = cudaMemsetAsync(L->bad, 0, 64, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cur, 0, sizeof(uint32_t) * n_cur, s);
+    if (e == cudaSuccess) {
+        validate_kernel<<<grid_for(n), threads, 0, s>>>(L->spec, L->bad, ctx->err_word);
+        norms_kernel<<<grid_for(n), threads, 0, s>>>(L->spec, L->sn, L->bad);
+        index_count_kernel<<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->bad);
+        index_scan_kernel<<<L->g.n_tiles, 1024, 0, s>>>(L->g, cur, L->tab, L->bad);
+        index_scatter_kernel<<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->ent,
+                                                                  L->bad);
+        e = cudaGetLastError();
+    }
+    uint32_t hbad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, L->bad, sizeof(uint32_t),
+                                              cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(cur);
+    if (e != cudaSuccess) {
+        library_free(L);
+        return cuda_fail(e, "cms_library_create");
+    }
+    if (hbad) {
+        library_free(L);
+        set_error("cms_library_create: invalid library spectra (offsets or peak counts)");
+        return CMS_ERR_DEVICE;
+    }
+    *out = L;
+    return CMS_OK;
+}
+
+extern "C" int cms_library_destroy(cms_library* lib) {
+    if (!lib) return CMS_OK;
+    cudaSetDevice(lib->device);
+    cudaDeviceSynchronize();
+    library_free(lib);
+    return CMS_OK;
+}
+
+extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const float* q_mz,
+                                  const double* q_a, const double* q_b, const int64_t* q_off,
+                                  int64_t n_q, int64_t n_q_peaks, float threshold,
+                                  int32_t* hit_ref, int32_t* hit_query, float* hit_score,
+                                  int32_t* hit_matches, uint8_t* hit_overflow, int64_t capacity,
+                                  int64_t* hit_count, void* stream) {
+    using namespace cms;
+    if (!ctx || !lib) {
+        set_error("cms_library_search: null context or library");
+        return CMS_ERR_INVALID;
+    }
+    if (ctx->device != lib->device) {
+        set_error("cms_library_search: context and library are on different devices");
+        return CMS_ERR_INVALID;
+    }
+    const SpecSet Q{q_mz, q_a, q_b, q_off, n_q, n_q_peaks};
+    if (!check_specset(Q, "query")) return CMS_ERR_INVALID;
+    if (!(threshold > 0.0f)) {
+        set_error("cms_library_search: threshold must be > 0");
+        return CMS_ERR_INVALID;
+    }
+    if (capacity < 0 || !hit_count || (capacity > 0 && (!hit_ref || !hit_query || !hit_score ||
+                                                        !hit_matches || !hit_overflow))) {
+        set_error("cms_library_search: invalid hit buffers");
+        return CMS_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    CMS_CUDA_TRY(cudaMemsetAsync(hit_count, 0, sizeof(int64_t), s));
+    if (n_q == 0) return CMS_OK;
+
+    const int cap = next_pow2(std::max(2, lib->match_limit));
+    const size_t pair_smem = (size_t)cap * 12 + 2 * 2048 * 4;
+    if (pair_smem > ctx->smem_optin) {
+        set_error("cms_library_search: match_limit too large for shared memory");
+        return CMS_ERR_UNSUPPORTED;
+    }
+    const long long items = (long long)n_q * lib->g.n_tiles;
+    const unsigned int spill_cap =
+        (unsigned int)std::min<long long>(std::max<long long>(1 << 16, items), 1 << 24);
+    const size_t gpool_warps = (size_t)ctx->sm_count * 64;
+    const size_t gpool_bytes = gpool_warps * (size_t)kGPool * 16;
+    size_t need = bump_size(64 * sizeof(uint64_t)) + bump_size(n_q * sizeof(double)) +
+                  bump_size(n_q * sizeof(int32_t)) + bump_size((size_t)spill_cap * sizeof(int2)) +
+                  bump_size(gpool_bytes) + 4096;
+    int rc = arena_reserve(ctx, ctx->scratch, need, s);
+    if (rc) return rc;
+    Bump bp{(char*)ctx->scratch.ptr, 0, ctx->scratch.bytes};
+    uint64_t* small = bp.take<uint64_t>(64);
+    uint32_t* bad = reinterpret_cast<uint32_t*>(small);
+    uint32_t* cls_count = reinterpret_cast<uint32_t*>(small + 1);
+    uint32_t* cls_cursor = reinterpret_cast<uint32_t*>(small + 10);
+    unsigned int* spill_count = reinterpret_cast<unsigned int*>(small + 20);
+    unsigned long long* work_join = reinterpret_cast<unsigned long long*>(small + 21);
+    unsigned long long* work_pair = reinterpret_cast<unsigned long long*>(small + 22);
+    double* snQ = bp.take<double>(n_q);
+    int32_t* order = bp.take<int32_t>(n_q);
+    int2* spill = bp.take<int2>(spill_cap);
+    unsigned char* gpool = bp.take<unsigned char>(gpool_bytes);
+    CMS_CUDA_TRY(cudaMemsetAsync(small, 0, 64 * sizeof(uint64_t), s));
+
+    const int threads = 256;
+    auto grid_for = [&](int64_t cnt) {
+        return (int)std::max<int64_t>(1, std::min<int64_t>((cnt + threads - 1) / threads,
+                                                           (int64_t)ctx->sm_count * 32));
+    };
+    {
+        StageScope sc(ctx, 0, 2, s);
+        validate_kernel<<<grid_for(n_q), threads, 0, s>>>(Q, bad, ctx->err_word);
+        norms_kernel<<<grid_for(n_q), threads, 0, s>>>(Q, snQ, bad);
+    }
+    {
+        StageScope sc(ctx, 1, 2, s);
+        order_count_kernel<<<grid_for(n_q), threads, 0, s>>>(Q, cls_count, bad);
+        order_scatter_kernel<<<grid_for(n_q), threads, 0, s>>>(Q, cls_count, cls_cursor, order,
+                                                               bad);
+    }
+    CMS_CUDA_TRY(cudaGetLastError());
+
+    SparseOut so{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
+                 reinterpret_cast<unsigned long long*>(hit_count), threshold};
+    JoinParams jp;
+    jp.A = Q;
+    jp.B = lib->spec;
+    jp.snA = snQ;
+    jp.snB = lib->sn;
+    jp.a_order = order;
+    jp.tab = lib->tab;
+    jp.ent = lib->ent;
+    jp.g = lib->g;
+    jp.tol = lib->tol;
+    jp.shift = lib->shift;
+    jp.match_limit = lib->match_limit;
+    jp.init_width_scale = 0.f;
+    if (lib->cand_per_pair > 0.0 && n_q > 0) {
+        const double mean_na = (double)n_q_peaks / (double)n_q;
+        const double lambda = lib->cand_per_pair / std::max(1.0, mean_na);
+        jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
+    }
+    jp.warp_smem_bytes = warp_slice_bytes(lib->g.tile);
+    jp.gpool = gpool;
+    jp.work = work_join;
+    jp.spill = SpillList{spill, spill_count, spill_cap};
+    jp.dense = DenseOut{nullptr, nullptr, nullptr, 0};
+    jp.sparse = so;
+    jp.err = ctx->err_word;
+    jp.bad = bad;
+    {
+        // a small batch takes only the CTAs it can keep busy, leaving the
+        // rest of the GPU to batches running concurrently on other streams
+        const int max_grid = (int)std::max<long long>(ctx->sm_count, (items + 63) / 64);
+        StageScope sc(ctx, 3, 1, s);
+        rc = launch_join<false, true, false>(ctx, jp, (size_t)jp.warp_smem_bytes * kJoinWarps,
+                                             gpool_warps, s, max_grid);
+        if (rc) return rc;
+    }
+    PairParams pp;
+    pp.R = lib->spec;
+    pp.Q = Q;
+    pp.snR = lib->sn;
+    pp.snQ = snQ;
+    pp.tol = lib->tol;
+    pp.shift = lib->shift;
+    pp.match_limit = lib->match_limit;
+    pp.cap = cap;
+    pp.pairs = spill;
+    pp.n_pairs = spill_count;
+    pp.pairs_cap = spill_cap;
+    pp.work = work_pair;
+    pp.dense = DenseOut{nullptr, nullptr, nullptr, 0};
+    pp.sparse = so;
+    pp.err = ctx->err_word;
+    pp.bad = bad;
+    {
+        StageScope sc(ctx, 4, 1, s);
+        CMS_CUDA_TRY(cudaFuncSetAttribute(pair_kernel<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)pair_smem));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<true>, 128, pair_smem);
+        pair_kernel<true><<<std::max(1, std::min(ctx->sm_count * std::max(1, per_sm),
+                                                  (int)std::min<long long>(spill_cap, 1 << 20))),
+                            128, pair_smem, s>>>(pp);
+    }
+    CMS_CUDA_TRY(cudaGetLastError());
     return CMS_OK;
 }

@@ -59,6 +59,13 @@ SIGNATURES = {
         _p, _p, _p, _p, c_int64, c_int64,
         c_double, c_double, c_int,
         _p, _p, _p, c_int64, _p, _p]),
+    "cms_library_create": (c_int, [
+        _p, _p, _p, _p, _p, c_int64, c_int64, c_double, c_double, c_int, _p,
+        POINTER(c_void_p), _p]),
+    "cms_library_search": (c_int, [
+        _p, _p, _p, _p, _p, _p, c_int64, c_int64, c_float,
+        _p, _p, _p, _p, _p, c_int64, _p, _p]),
+    "cms_library_destroy": (c_int, [_p]),
     "cms_profile_enable": (c_int, [_p, c_int]),
     "cms_profile_read": (c_int, [_p, _p, _p, c_int]),
     "cms_fingerprint": (c_int, [

@@ -45,6 +45,27 @@ def _sort_within(mz: np.ndarray, seg: np.ndarray) -> np.ndarray:
     return mz[order]
 
 
+def sorted_uniform(rng, lengths: np.ndarray, lo: float, hi: float) -> np.ndarray:
+    """Ascending U(lo, hi) samples per spectrum in O(P): the order statistics of
+    n uniforms are the normalised partial sums of n + 1 exponential spacings."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    n = lengths.shape[0]
+    ext = lengths + 1
+    e = rng.exponential(1.0, int(ext.sum()))
+    c = np.cumsum(e)
+    ends = np.cumsum(ext) - 1
+    starts = ends - lengths
+    base = np.where(starts > 0, c[np.maximum(starts - 1, 0)], 0.0)
+    total = c[ends] - base
+    seg = np.repeat(np.arange(n), lengths)
+    # output j of segment s is the partial sum at index starts[s] + j
+    first_out = np.concatenate([[0], np.cumsum(lengths)[:-1]])
+    within = np.arange(int(lengths.sum())) - first_out[seg]
+    pos = starts[seg] + within
+    u = (c[pos] - base[seg]) / total[seg]
+    return (lo + (hi - lo) * u).astype(np.float32)
+
+
 def _scale_to_max(x: np.ndarray, off: np.ndarray) -> np.ndarray:
     nonempty = off[1:] > off[:-1]
     mx = np.ones(off.shape[0] - 1, dtype=x.dtype)
@@ -54,9 +75,10 @@ def _scale_to_max(x: np.ndarray, off: np.ndarray) -> np.ndarray:
     return (x / np.repeat(mx, lengths)).astype(np.float32)
 
 
-def _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power) -> PackedSpectra:
+def _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power,
+           presorted: bool = False) -> PackedSpectra:
     off, seg = _segments(lengths)
-    mz = _sort_within(mz.astype(np.float32), seg)
+    mz = mz.astype(np.float32) if presorted else _sort_within(mz.astype(np.float32), seg)
     inten = _scale_to_max(inten.astype(np.float32), off)
     return pack_csr(mz, inten, off, n_max_peaks, mz_power, intensity_power, check=False)
 
@@ -66,9 +88,9 @@ def uniform_spectra(n: int, seed: int = 0, n_max_peaks: int = 1024, mz_power: fl
     rng = np.random.default_rng(seed)
     lengths = rng.integers(10, 201, n).astype(np.int64)
     p = int(lengths.sum())
-    mz = rng.uniform(50.0, 1000.0, p)
+    mz = sorted_uniform(rng, lengths, 50.0, 1000.0)
     inten = 1.0 - rng.uniform(0.0, 1.0, p)  # (0, 1]
-    return _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power)
+    return _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power, presorted=True)
 
 
 def lognormal_lengths(rng, n: int, median: float = 60.0, sigma: float = LOGNORMAL_SIGMA,
@@ -81,9 +103,9 @@ def lognormal_spectra(n: int, seed: int = 0, n_max_peaks: int = 1024, mz_power: 
     rng = np.random.default_rng(seed)
     lengths = lognormal_lengths(rng, n, sigma=sigma)
     p = int(lengths.sum())
-    mz = rng.uniform(50.0, 2000.0, p)
+    mz = sorted_uniform(rng, lengths, 50.0, 2000.0)
     inten = rng.exponential(1.0, p)
-    return _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power)
+    return _build(lengths, mz, inten, n_max_peaks, mz_power, intensity_power, presorted=True)
 
 
 def cluster_centres(seed: int = 12345, n_centres: int = 200) -> np.ndarray:

@@ -178,6 +178,33 @@ int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* re
                              void* stream);
 
 /*
+ * Resident library: a spectrum set indexed once on the device (the "reference"
+ * side of matchms, e.g. a spectral library) and searched by many query
+ * batches.  This is the served form of CudaCosineGreedy.matrix(library,
+ * queries, array_type="sparse") (CudaCosineGreedy.py:186-226): each search
+ * returns every (library spectrum, query) pair with score >= threshold, with
+ * the same numerics as cms_cosine_greedy.  The library's spectrum arrays stay
+ * owned by the caller and must outlive the library object; the index and the
+ * library norms are allocated by cms_library_create (which synchronises
+ * `stream`) and freed by cms_library_destroy.  cfg (may be NULL) sets the
+ * library tile size / bucket width and the expected candidates per pair.
+ * Searches on different contexts and streams may run concurrently against
+ * one library (it is read-only after creation).  Hit buffers and hit_count
+ * follow cms_cosine_greedy_sparse (hit_ref = library index, hit_query =
+ * query index).
+ */
+int cms_library_create(cms_ctx* ctx, const float* mz, const double* a, const double* b,
+                       const int64_t* off, int64_t n, int64_t n_peaks, double tolerance,
+                       double shift, int match_limit, const cms_cosine_config* cfg,
+                       cms_library** out, void* stream);
+int cms_library_search(cms_ctx* ctx, const cms_library* lib, const float* q_mz,
+                       const double* q_a, const double* q_b, const int64_t* q_off, int64_t n_q,
+                       int64_t n_q_peaks, float threshold, int32_t* hit_ref, int32_t* hit_query,
+                       float* hit_score, int32_t* hit_matches, uint8_t* hit_overflow,
+                       int64_t capacity, int64_t* hit_count, void* stream);
+int cms_library_destroy(cms_library* lib);
+
+/*
  * Allocation-free greedy cosine, dense output.  No counterpart in the
  * reference: this entry point exists for callers that must not have a
  * library allocate device memory -- an application whose GPU memory is
