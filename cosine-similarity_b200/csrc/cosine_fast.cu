@@ -47,6 +47,7 @@ constexpr int kJoinWarps = 8;
 constexpr int kJoinThreads = kJoinWarps * 32;
 constexpr int kPool = 256;        // candidate pool entries per warp
 constexpr int kLongRun = 32;      // longer runs go to the pair kernel
+constexpr int kMidRun = 8;        // runs up to this length are resolved four per warp step
 constexpr int kMaxTile = 4096;    // max query spectra per tile
 constexpr int kOrderClasses = 17; // log2 length classes (0..16)
 
@@ -307,6 +308,7 @@ struct JoinParams {
 constexpr int kFetch = 4;  // work items taken per atomic
 constexpr int kPoolMax = 4096;             // candidates per sweep: smem pool + global extension
 constexpr int kGPool = kPoolMax - kPool;   // global extension entries per warp
+static_assert(kPoolMax <= 4096, "queued run starts are packed into 12 bits");
 
 // A warp's candidate pool: the first kPool entries live in shared memory, the
 // rest in a per-warp slice of global scratch (L2-resident), so that a large
@@ -366,7 +368,9 @@ struct Pool {
 //                          scatter) ends of each query's run in perm
 //   n     int              candidates pushed in this sweep
 //   res   int2   [32]      per-lane staging of run results
-//   long  uint16 [kLongRuns] starts of runs longer than 2 (resolved by the warp)
+//   long  uint16 [kLongRuns] runs longer than 2 (resolved by the warp): runs of
+//                          3..kMidRun candidates from the front, longer ones
+//                          from the back
 constexpr int kLongRuns = 64;
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
     // counters: tile/2 + 1 words are used; the 16-byte zeroing may touch up
@@ -670,72 +674,142 @@ join_kernel(JoinParams P) {
             // where the query index changes.  The result of a run is packed
             // into the ckey slot of its first candidate: (score f32 bits,
             // matches), matches = -1 for a pair sent to the pair kernel.
-            int n_long = 0;
-            // long runs: warp bitonic sort of (key, gen) descending in
-            // registers, then greedy by ballot (leaders in sorted order)
+            // Queued runs of 3..32 candidates share the long_runs list: runs of
+            // at most kMidRun candidates from the front (start | (L-1) << 12),
+            // longer ones from the back (start only).
+            int n_mid = 0, n_big = 0;
             auto flush_long = [&]() {
-            for (int r = 0; r < n_long; ++r) {
-                const int i0 = long_runs[r];
-                const int q0 = pool.cq(pool.perm(i0));
-                const int L = (int)cnt_get(cnt, q0) - i0;
-                double k = -INFINITY;
-                uint32_t g = 0;
-                if (lane < L) {
-                    const int sl = pool.perm(i0 + lane);
-                    k = pool.key(sl);
-                    g = pool.gen(sl);
-                }
+                __syncwarp();
+                // runs of 3..8 candidates, four at a time: each 8-lane segment
+                // sorts one run's (key, gen) descending in registers (bitonic),
+                // then resolves it greedily by segment-wise ballot
+                const int seg = lane >> 3, t = lane & 7;
+                for (int r = 0; r < n_mid; r += 4) {
+                    const bool valid = r + seg < n_mid;
+                    const unsigned e = valid ? (unsigned)long_runs[r + seg] : 0u;
+                    const int i0 = (int)(e & 0xFFFu);
+                    const int L = valid ? (int)(e >> 12) + 1 : 0;
+                    double k = -INFINITY;
+                    uint32_t g = 0;
+                    int sl = 0;
+                    if (t < L) {
+                        sl = pool.perm(i0 + t);
+                        k = pool.key(sl);
+                        g = pool.gen(sl);
+                    }
 #pragma unroll
-                for (int kk = 2; kk <= 32; kk <<= 1) {
+                    for (int kk = 2; kk <= kMidRun; kk <<= 1) {
 #pragma unroll
-                    for (int j = kk >> 1; j > 0; j >>= 1) {
-                        const double ok = __shfl_xor_sync(full, k, j);
-                        const uint32_t og = __shfl_xor_sync(full, g, j);
-                        const bool lower = (lane & j) == 0;
-                        const bool desc = (lane & kk) == 0;
-                        // the lower lane of a descending pair keeps the larger
-                        const bool mine_first = before(k, g, ok, og);
-                        const bool keep = (lower == desc) ? mine_first : !mine_first;
-                        if (!keep) {
-                            k = ok;
-                            g = og;
+                        for (int j = kk >> 1; j > 0; j >>= 1) {
+                            const double ok = __shfl_xor_sync(full, k, j);
+                            const uint32_t og = __shfl_xor_sync(full, g, j);
+                            const bool lower = (t & j) == 0;
+                            const bool desc = (t & kk) == 0;
+                            const bool mine_first = before(k, g, ok, og);
+                            const bool keep = (lower == desc) ? mine_first : !mine_first;
+                            if (!keep) {
+                                k = ok;
+                                g = og;
+                            }
+                        }
+                    }
+                    bool alive = t < L;
+                    unsigned bal = __ballot_sync(full, alive);
+                    double score = 0.0;
+                    int mt = 0;
+                    while (bal) {
+                        const unsigned mine = (bal >> (seg * 8)) & 0xFFu;
+                        const int leader = mine ? seg * 8 + __ffs(mine) - 1 : lane;
+                        const uint32_t lg = __shfl_sync(full, g, leader);
+                        const double lk = __shfl_sync(full, k, leader);
+                        if (mine) {
+                            score = __dadd_rn(score, lk);
+                            ++mt;
+                            if (lane == leader || ((g >> 16) == (lg >> 16)) ||
+                                ((g & 0xFFFFu) == (lg & 0xFFFFu)))
+                                alive = false;
+                        }
+                        bal = __ballot_sync(full, alive);
+                    }
+                    if (valid && t == 0) {
+                        // sl is still the slot of the run's first candidate:
+                        // the sort moved keys and gens only
+                        const int q0 = pool.cq(sl);
+                        const int bq = b_begin + range_lo + q0;
+                        const double snB = P.snB[bq];
+                        const float sc = (float)__ddiv_rn(
+                            score, A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA));
+                        if (SPARSE) {
+                            if (sc >= P.sparse.threshold)
+                                emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
+                        } else {
+                            pool.set_result(sl, make_int2(__float_as_int(sc), mt));
                         }
                     }
                 }
-                bool alive = lane < L;
-                unsigned bal = __ballot_sync(full, alive);
-                double score = 0.0;
-                int mt = 0;
-                while (bal) {
-                    const int leader = __ffs(bal) - 1;
-                    const uint32_t lg = __shfl_sync(full, g, leader);
-                    const double lk = __shfl_sync(full, k, leader);
-                    score = __dadd_rn(score, lk);
-                    ++mt;
-                    if (lane == leader ||
-                        ((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu)))
-                        alive = false;
-                    bal = __ballot_sync(full, alive);
-                }
-                if (lane == 0) {
-                    const int bq = b_begin + range_lo + q0;
-                    const double snB = P.snB[bq];
-                    const float sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
-                                                                      : __dmul_rn(snB, snA));
-                    if (SPARSE) {
-                        if (sc >= P.sparse.threshold)
-                            emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
-                    } else {
-                        pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                // runs of 9..32 candidates, one at a time on the whole warp
+                for (int r = 0; r < n_big; ++r) {
+                    const int i0 = long_runs[kLongRuns - 1 - r];
+                    const int q0 = pool.cq(pool.perm(i0));
+                    const int L = (int)cnt_get(cnt, q0) - i0;
+                    double k = -INFINITY;
+                    uint32_t g = 0;
+                    if (lane < L) {
+                        const int sl = pool.perm(i0 + lane);
+                        k = pool.key(sl);
+                        g = pool.gen(sl);
+                    }
+#pragma unroll
+                    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+                        for (int j = kk >> 1; j > 0; j >>= 1) {
+                            const double ok = __shfl_xor_sync(full, k, j);
+                            const uint32_t og = __shfl_xor_sync(full, g, j);
+                            const bool lower = (lane & j) == 0;
+                            const bool desc = (lane & kk) == 0;
+                            // the lower lane of a descending pair keeps the larger
+                            const bool mine_first = before(k, g, ok, og);
+                            const bool keep = (lower == desc) ? mine_first : !mine_first;
+                            if (!keep) {
+                                k = ok;
+                                g = og;
+                            }
+                        }
+                    }
+                    bool alive = lane < L;
+                    unsigned bal = __ballot_sync(full, alive);
+                    double score = 0.0;
+                    int mt = 0;
+                    while (bal) {
+                        const int leader = __ffs(bal) - 1;
+                        const uint32_t lg = __shfl_sync(full, g, leader);
+                        const double lk = __shfl_sync(full, k, leader);
+                        score = __dadd_rn(score, lk);
+                        ++mt;
+                        if (lane == leader ||
+                            ((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu)))
+                            alive = false;
+                        bal = __ballot_sync(full, alive);
+                    }
+                    if (lane == 0) {
+                        const int bq = b_begin + range_lo + q0;
+                        const double snB = P.snB[bq];
+                        const float sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
+                                                                          : __dmul_rn(snB, snA));
+                        if (SPARSE) {
+                            if (sc >= P.sparse.threshold)
+                                emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
+                        } else {
+                            pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                        }
                     }
                 }
                 __syncwarp();
-            }
-            n_long = 0;
+                n_mid = 0;
+                n_big = 0;
             };
             // Runs of length 1 and 2 are resolved by their lane in closed
-            // form; longer runs (up to 32) are queued and resolved one at a
-            // time by the whole warp.
+            // form; longer runs (up to 32) are queued and resolved by the warp.
             for (int c = 0; c < n; c += 32) {
                 const int i = c + lane;
                 bool st = false;
@@ -747,10 +821,17 @@ join_kernel(JoinParams P) {
                 int L = 0;
                 if (st) L = (int)cnt_get(cnt, q_i) - i;
                 const bool is_long = st && L > 2 && L <= kLongRun && L < P.match_limit;
-                const unsigned lb = __ballot_sync(full, is_long);
-                if (n_long + __popc(lb) > kLongRuns) flush_long();
-                if (is_long) long_runs[n_long + __popc(lb & ((1u << lane) - 1u))] = (uint16_t)i;
-                n_long += __popc(lb);
+                const bool is_mid = is_long && L <= kMidRun;
+                const unsigned mb = __ballot_sync(full, is_mid);
+                const unsigned bb = __ballot_sync(full, is_long && !is_mid);
+                if (n_mid + n_big + __popc(mb) + __popc(bb) > kLongRuns) flush_long();
+                const unsigned below = (1u << lane) - 1u;
+                if (is_mid)
+                    long_runs[n_mid + __popc(mb & below)] = (uint16_t)(i | ((L - 1) << 12));
+                else if (is_long)
+                    long_runs[kLongRuns - 1 - (n_big + __popc(bb & below))] = (uint16_t)i;
+                n_mid += __popc(mb);
+                n_big += __popc(bb);
                 if (st && !is_long) {
                     const int bq = b_begin + range_lo + q_i;
                     float sc;
