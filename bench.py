@@ -423,6 +423,9 @@ def other_workloads(dev, args):
         ms = _time_ms(lambda: kernels.fingerprint_matrix(m, rb, None, qb, None, 64, float("nan"),
                                                          out=fout))
         fp[m] = n_fp * n_fp / (ms / 1e3)
+    # is_symmetric=True on one set: upper triangle + mirror copy
+    ms_sym = _time_ms(lambda: kernels.fingerprint_matrix("jaccard", rb, None, rb, None, 64,
+                                                         float("nan"), out=fout, symmetric=True))
     del fout
     torch.cuda.empty_cache()
     # the reference's own torch formulation (float32 GEMM + elementwise) on a 20k tile
@@ -449,7 +452,31 @@ def other_workloads(dev, args):
                      "peak_popc64_per_s": popc_peak, "frac": 32 * fp["jaccard"] / popc_peak,
                      "hbm_frac": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
         "reference_torch_cuda_jaccard_pairs_per_s": nt * nt / (tms / 1e3),
-        "reference_torch_sample": f"{nt} x {nt}"}
+        "reference_torch_sample": f"{nt} x {nt}",
+        "symmetric_jaccard_output_pairs_per_s": n_fp * n_fp / (ms_sym / 1e3)}
+
+    # is_symmetric=True greedy cosine on one set of the headline distribution:
+    # upper triangle + mirror copy, against the full matrix of the same set
+    n_sym = min(args.n, 40_000)
+    sset = synthetic.lognormal_spectra(n_sym, seed=args.seed + 5)
+    s_cfg = autotune.choose_config(sset, sset, TOL)
+    sd = sset.to_device(dev)
+    sout = tuple(torch.empty((n_sym, n_sym), dtype=t, device=dev)
+                 for t in (torch.float32, torch.int32, torch.uint8))
+    ms_full = _time_ms(lambda: kernels.cosine_greedy_dense(sd, sd, TOL, 0.0, MATCH_LIMIT,
+                                                            out=sout, config=s_cfg), reps=2)
+    ms_half = _time_ms(lambda: kernels.cosine_greedy_dense(sd, sd, TOL, 0.0, MATCH_LIMIT,
+                                                            out=sout,
+                                                            config=dict(s_cfg, symmetric=1)),
+                       reps=2)
+    res["symmetric_cosine_40k"] = {
+        "workload": f"{n_sym} x {n_sym}, one set (lognormal peaks, tol 0.01), is_symmetric",
+        "full_output_pairs_per_s": n_sym * n_sym / (ms_full / 1e3),
+        "symmetric_output_pairs_per_s": n_sym * n_sym / (ms_half / 1e3),
+        "full_ms": ms_full, "symmetric_ms": ms_half}
+    del sout, sd
+    sset._device.clear()
+    torch.cuda.empty_cache()
 
     # 1024 x 1024 uniform spectra, tol 0.1 (the reference's CPU-runnable case)
     u_r = synthetic.uniform_spectra(1024, seed=args.seed + 1).to_device(dev)

@@ -54,7 +54,15 @@ struct SparseOut {
     int64_t capacity;
     unsigned long long* count;  // int64 count, as an atomically updatable word
     float threshold;
+    int mirror;                 // nonzero: every hit (r, q) with r != q also as (q, r)
 };
+
+// Symmetric dense output: copies element (c, r) to (r, c) for every r > c of
+// the n x n matrix (score, and matches/overflow unless null), reading the
+// upper triangle and writing the lower one.  `bad` (may be null) is a device
+// flag that turns the kernel into a no-op.  Defined in mirror.cu.
+int launch_mirror(const DenseOut& d, int64_t n, const uint32_t* bad, int sm_count,
+                  cudaStream_t s);
 
 // Thread-local last-error string.
 void set_error(const char* fmt, ...);

@@ -255,13 +255,21 @@ __device__ __forceinline__ bool before(double k1, uint32_t g1, double k2, uint32
 
 __device__ __forceinline__ void emit_hit(const SparseOut& o, int r, int q, float sc, int mt,
                                          uint8_t ovf) {
-    const unsigned long long pos = atomicAdd(o.count, 1ull);
+    const bool both = o.mirror && r != q;
+    const unsigned long long pos = atomicAdd(o.count, both ? 2ull : 1ull);
     if (pos < (unsigned long long)o.capacity) {
         o.r[pos] = r;
         o.q[pos] = q;
         o.score[pos] = sc;
         o.matches[pos] = mt;
         o.overflow[pos] = ovf;
+    }
+    if (both && pos + 1 < (unsigned long long)o.capacity) {
+        o.r[pos + 1] = q;
+        o.q[pos + 1] = r;
+        o.score[pos + 1] = sc;
+        o.matches[pos + 1] = mt;
+        o.overflow[pos + 1] = ovf;
     }
 }
 
@@ -303,6 +311,7 @@ struct JoinParams {
     SparseOut sparse;
     uint32_t* err;
     const uint32_t* bad;
+    int sym;  // only pairs (reference i, query j) with i <= j
 };
 
 constexpr int kFetch = 4;  // work items taken per atomic
@@ -506,9 +515,17 @@ join_kernel(JoinParams P) {
         int width = tn;
         if (P.init_width_scale > 0.f && na > 0)
             width = max(32, min(tn, (int)(P.init_width_scale / (float)na)));
-        int range_lo = 0;
-        while (range_lo < tn) {
-            const int range_hi = min(range_lo + width, tn);
+        // queries of this item: the whole tile, or under `sym` those on or
+        // above the diagonal (reference index <= query index)
+        int range_lo = 0, q_end = tn;
+        if (P.sym) {
+            if (A_IS_REF)
+                range_lo = max(0, min(tn, a - b_begin));
+            else
+                q_end = max(0, min(tn, a - b_begin + 1));
+        }
+        while (range_lo < q_end) {
+            const int range_hi = min(range_lo + width, q_end);
             const int rw = range_hi - range_lo;
             // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
             for (int w = 4 * lane; w < rw / 2 + 2; w += 128)
@@ -966,6 +983,7 @@ struct PairParams {
     SparseOut sparse;
     uint32_t* err;
     const uint32_t* bad;
+    int sym;  // only pairs (reference i, query j) with i <= j
 };
 
 template <bool SPARSE>
@@ -1001,6 +1019,7 @@ __global__ void pair_kernel(PairParams P) {
         } else {
             ri = item / P.Q.n;
             qi = item - ri * P.Q.n;
+            if (P.sym && ri > qi) continue;  // the lower triangle is copied afterwards
         }
         const int64_t r0 = P.R.off[ri], q0 = P.Q.off[qi];
         const int nr = (int)(P.R.off[ri + 1] - r0), nq = (int)(P.Q.off[qi + 1] - q0);
@@ -1249,6 +1268,12 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     Plan p;
     int rc = make_plan(args, cfg, sparse != nullptr, p);
     if (rc) return rc;
+    const int sym = (cfg && cfg->symmetric) ? 1 : 0;
+    if (sym && args.ref.n != args.qry.n) {
+        set_error("cms_cosine_greedy: symmetric needs as many queries as references "
+                  "(%lld != %lld)", (long long)args.ref.n, (long long)args.qry.n);
+        return CMS_ERR_INVALID;
+    }
     const size_t pair_smem = (size_t)p.cap * 12 + 2 * 2048 * 4;
     if (pair_smem > ctx->smem_optin) {
         set_error("cms_cosine_greedy: match_limit %d needs %zu B shared memory (> %zu)",
@@ -1304,7 +1329,7 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
 
     if (sparse) CMS_CUDA_TRY(cudaMemsetAsync(sparse->count, 0, sizeof(unsigned long long), s));
 
-    PairParams pp;
+    PairParams pp{};
     pp.R = args.ref;
     pp.Q = args.qry;
     pp.snR = snR;
@@ -1319,8 +1344,16 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     pp.work = work_pair;
     pp.dense = dense ? *dense : DenseOut{nullptr, nullptr, nullptr, 0};
     pp.sparse = sparse ? *sparse : SparseOut{};
+    pp.sparse.mirror = sym;
     pp.err = ctx->err_word;
     pp.bad = bad;
+    pp.sym = sym;
+    // dense symmetric output: the lower triangle is copied from the upper
+    // one once every pair kernel has written it
+    auto mirror = [&]() -> int {
+        if (!sym || sparse) return CMS_OK;
+        return launch_mirror(pp.dense, nR, bad, ctx->sm_count, s);
+    };
 
     int pair_blocks_per_sm = 1;
     if (sparse) {
@@ -1342,7 +1375,7 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         else
             pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
         CMS_CUDA_TRY(cudaGetLastError());
-        return CMS_OK;
+        return mirror();
     }
 
     // ---- mode 1: order, index, join, spill ----
@@ -1370,7 +1403,7 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     }
     CMS_CUDA_TRY(cudaGetLastError());
 
-    JoinParams jp;
+    JoinParams jp{};
     jp.A = args.ref;
     jp.B = args.qry;
     jp.snA = snR;
@@ -1397,6 +1430,7 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.sparse = pp.sparse;
     jp.err = ctx->err_word;
     jp.bad = bad;
+    jp.sym = sym;
     const size_t join_smem = (size_t)warp_slice_bytes(p.tile) * kJoinWarps;
     {
         StageScope sc(ctx, 3, 1, s);
@@ -1412,13 +1446,15 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     pp.pairs = spill;
     pp.n_pairs = spill_count;
     pp.pairs_cap = p.spill_cap;
-    StageScope sc(ctx, 4, 1, s);
-    if (sparse)
-        pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
-    else
-        pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
-    CMS_CUDA_TRY(cudaGetLastError());
-    return CMS_OK;
+    {
+        StageScope sc(ctx, 4, 1, s);
+        if (sparse)
+            pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        else
+            pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        CMS_CUDA_TRY(cudaGetLastError());
+    }
+    return mirror();
 }
 
 bool check_common(const CosineArgs& a, const char* who) {
@@ -1614,7 +1650,7 @@ extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_
     norms_kernel<<<grid_for(n_q), threads, 0, s>>>(args.qry, snQ, bad);
     CMS_CUDA_TRY(cudaGetLastError());
 
-    PairParams pp;
+    PairParams pp{};
     pp.R = args.ref;
     pp.Q = args.qry;
     pp.snR = snR;
@@ -1854,7 +1890,7 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
 
     SparseOut so{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
                  reinterpret_cast<unsigned long long*>(hit_count), threshold};
-    JoinParams jp;
+    JoinParams jp{};
     jp.A = Q;
     jp.B = lib->spec;
     jp.snA = snQ;
@@ -1889,7 +1925,7 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
                                              gpool_warps, s, max_grid);
         if (rc) return rc;
     }
-    PairParams pp;
+    PairParams pp{};
     pp.R = lib->spec;
     pp.Q = Q;
     pp.snR = lib->sn;

@@ -37,6 +37,7 @@ struct FpParams {
     float fill;
     float* out;
     int64_t ld;
+    int sym;  // only outputs (i, j) with i <= j (n_r == n_q)
 };
 
 __device__ __forceinline__ uint64_t load_word64(const uint32_t* row, int w64, int n_words) {
@@ -63,6 +64,8 @@ __device__ __forceinline__ float measure_of(int inter, int a, int b) {
 template <int MEASURE>
 __global__ void __launch_bounds__(kFpThreads)
 fingerprint_kernel(FpParams P) {
+    // symmetric: tiles wholly below the diagonal are copied afterwards
+    if (P.sym && blockIdx.y > blockIdx.x) return;
     extern __shared__ __align__(16) uint64_t fp_smem[];
     uint64_t* sR = fp_smem;
     uint64_t* sQ = fp_smem + kBM * kLd;
@@ -140,7 +143,7 @@ fingerprint_kernel(FpParams P) {
         for (int j = 0; j < 8; ++j) {
             const int cc = tc + 16 * j;
             const int64_t gc = col0 + cc;
-            if (gc >= P.n_q) continue;
+            if (gc >= P.n_q || (P.sym && gr > gc)) continue;
             const bool qv = P.q_valid ? P.q_valid[gc] != 0 : true;
             orow[gc] = (rv && qv) ? measure_of<MEASURE>(acc[i][j], pa[rr], pb[cc]) : P.fill;
         }
@@ -157,30 +160,32 @@ void launch_fp(dim3 grid, size_t smem, cudaStream_t s, const FpParams& P) {
 }  // namespace
 }  // namespace cms
 
-extern "C" int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
-                               int64_t n_ref, const uint32_t* q_bits, const uint8_t* q_valid,
-                               int64_t n_q, int n_words, float fill, float* out, int64_t ld,
-                               void* stream) {
-    using namespace cms;
+namespace cms {
+namespace {
+
+int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
+                     const uint8_t* ref_valid, int64_t n_ref, const uint32_t* q_bits,
+                     const uint8_t* q_valid, int64_t n_q, int n_words, float fill, float* out,
+                     int64_t ld, int sym, void* stream) {
     if (measure < CMS_FP_JACCARD || measure > CMS_FP_COSINE) {
-        set_error("cms_fingerprint: unknown measure %d", measure);
+        set_error("%s: unknown measure %d", who, measure);
         return CMS_ERR_INVALID;
     }
     if (n_ref < 0 || n_q < 0 || n_words < 0 || n_words > 1024 || ld < n_q) {
-        set_error("cms_fingerprint: invalid sizes (n_words must be in [0, 1024], ld >= n_q)");
+        set_error("%s: invalid sizes (n_words must be in [0, 1024], ld >= n_q)", who);
         return CMS_ERR_INVALID;
     }
     if (n_ref == 0 || n_q == 0) return CMS_OK;
     if (!out || (n_words > 0 && (!ref_bits || !q_bits))) {
-        set_error("cms_fingerprint: null pointer");
+        set_error("%s: null pointer", who);
         return CMS_ERR_INVALID;
     }
     const int64_t gy = (n_ref + kBM - 1) / kBM, gx = (n_q + kBN - 1) / kBN;
     if (gy > 65535 || gx > 2147483647LL) {
-        set_error("cms_fingerprint: too many rows for one launch (split the reference side)");
+        set_error("%s: too many rows for one launch (split the reference side)", who);
         return CMS_ERR_UNSUPPORTED;
     }
-    FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld};
+    FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld, sym};
     dim3 grid((unsigned)gx, (unsigned)gy);
     cudaStream_t s = (cudaStream_t)stream;
     const size_t smem = (size_t)(kBM + kBN) * kLd * sizeof(uint64_t);
@@ -196,5 +201,30 @@ extern "C" int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint
             break;
     }
     CMS_CUDA_TRY(cudaGetLastError());
+    if (sym) {
+        int dev = 0, sms = 148;
+        CMS_CUDA_TRY(cudaGetDevice(&dev));
+        CMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        return launch_mirror(DenseOut{out, nullptr, nullptr, ld}, n_ref, nullptr, sms, s);
+    }
     return CMS_OK;
+}
+
+}  // namespace
+}  // namespace cms
+
+extern "C" int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
+                               int64_t n_ref, const uint32_t* q_bits, const uint8_t* q_valid,
+                               int64_t n_q, int n_words, float fill, float* out, int64_t ld,
+                               void* stream) {
+    return cms::fingerprint_impl("cms_fingerprint", measure, ref_bits, ref_valid, n_ref, q_bits,
+                                 q_valid, n_q, n_words, fill, out, ld, 0, stream);
+}
+
+extern "C" int cms_fingerprint_symmetric(int measure, const uint32_t* ref_bits,
+                                         const uint8_t* ref_valid, const uint32_t* q_bits,
+                                         const uint8_t* q_valid, int64_t n, int n_words,
+                                         float fill, float* out, int64_t ld, void* stream) {
+    return cms::fingerprint_impl("cms_fingerprint_symmetric", measure, ref_bits, ref_valid, n,
+                                 q_bits, q_valid, n, n_words, fill, out, ld, 1, stream);
 }

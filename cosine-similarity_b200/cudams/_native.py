@@ -70,6 +70,8 @@ SIGNATURES = {
     "cms_profile_read": (c_int, [_p, _p, _p, c_int]),
     "cms_fingerprint": (c_int, [
         c_int, _p, _p, c_int64, _p, _p, c_int64, c_int, c_float, _p, c_int64, _p]),
+    "cms_fingerprint_symmetric": (c_int, [
+        c_int, _p, _p, _p, _p, c_int64, c_int, c_float, _p, c_int64, _p]),
 }
 
 
@@ -82,7 +84,7 @@ class NativeError(RuntimeError):
 
 
 class CosineConfig(ctypes.Structure):
-    """cms_cosine_config (zero fields = automatic)."""
+    """cms_cosine_config (zero fields = automatic; symmetric=1 computes i <= j only)."""
 
     _fields_ = [
         ("tile_spectra", c_int32),
@@ -91,6 +93,7 @@ class CosineConfig(ctypes.Structure):
         ("mode", c_int32),
         ("pair_threads", c_int32),
         ("cand_per_pair", c_double),
+        ("symmetric", c_int32),
     ]
 
 

@@ -170,14 +170,26 @@ def cosine_greedy_sparse(ref: DeviceSpectra, qry: DeviceSpectra, tolerance: floa
 
 
 def fingerprint_matrix(measure: str, r_bits, r_valid, q_bits, q_valid, n_words: int, fill: float,
-                       *, out=None, stream=None):
-    """Fingerprint similarity [n_ref, n_q] float32 on the device."""
+                       *, out=None, stream=None, symmetric: bool = False):
+    """Fingerprint similarity [n_ref, n_q] float32 on the device.
+
+    symmetric: n_ref == n_q; only pairs (i, j) with i <= j are computed and
+    (j, i) gets the same value (matchms is_symmetric=True)."""
     lib = _native.load()
     device = r_bits.device
     s = _stream(device, stream)
     n_r, n_q = int(r_bits.shape[0]), int(q_bits.shape[0])
+    if symmetric and n_r != n_q:
+        raise ValueError(f"symmetric fingerprint matrix needs n_ref == n_q ({n_r} != {n_q})")
     if out is None:
         out = torch.empty((n_r, n_q), dtype=torch.float32, device=device)
+    if symmetric:
+        rc = lib.cms_fingerprint_symmetric(_native.FP_MEASURES[measure], ptr(r_bits),
+                                           ptr(r_valid), ptr(q_bits), ptr(q_valid), n_r,
+                                           int(n_words), float(fill), ptr(out),
+                                           int(out.stride(0)), stream_handle(s))
+        check(rc, "cms_fingerprint_symmetric")
+        return out
     rc = lib.cms_fingerprint(_native.FP_MEASURES[measure], ptr(r_bits), ptr(r_valid), n_r,
                              ptr(q_bits), ptr(q_valid), n_q, int(n_words), float(fill), ptr(out),
                              int(out.stride(0)), stream_handle(s))

@@ -140,8 +140,11 @@ class CudaCosineGreedy(BaseSimilarity):
         rows = max(1, int(budget // max(1, n_q * _BYTES_PER_PAIR)))
         return max(min(n_ref, rows), min(n_ref, int(self.batch_size or 1)))
 
-    def _compute(self, ref: PackedSpectra, qry: PackedSpectra):
-        """Dense result on the host: (score, matches, overflow) [n_ref, n_q]."""
+    def _compute(self, ref: PackedSpectra, qry: PackedSpectra, symmetric: bool = False):
+        """Dense result on the host: (score, matches, overflow) [n_ref, n_q].
+
+        symmetric: only pairs (i, j) with i <= j are computed and (j, i) gets
+        the same result (matchms is_symmetric=True; needs n_ref == n_q)."""
         import torch
 
         dev = self._torch_device()
@@ -153,9 +156,14 @@ class CudaCosineGreedy(BaseSimilarity):
         if R == 0 or Q == 0:
             return score, matches, overflow
         cfg = self._config_for(ref, qry)
-        qd = qry.to_device(dev)
         rows = self._row_block(R, Q, dev)
         stream = torch.cuda.current_stream(dev)
+        if symmetric and rows < R:
+            return self._compute_symmetric_blocked(ref, qry, cfg, rows, dev, stream,
+                                                   (score, matches, overflow))
+        if symmetric:
+            cfg = dict(cfg, symmetric=1)
+        qd = qry.to_device(dev)
         bufs = None
         for r0 in range(0, R, rows):
             r1 = min(R, r0 + rows)
@@ -175,6 +183,43 @@ class CudaCosineGreedy(BaseSimilarity):
             overflow[r0:r1] = bufs[2].cpu().numpy()
         return score, matches, overflow
 
+    def _compute_symmetric_blocked(self, ref, qry, cfg, rows, dev, stream, out):
+        """Symmetric result when the matrix does not fit the device at once:
+        row block [r0, r1) computes its diagonal square symmetrically and the
+        columns right of it fully; the columns left of r0 are the transpose of
+        blocks already computed."""
+        import torch
+
+        score, matches, overflow = out
+        R = ref.n
+        for r0 in range(0, R, rows):
+            r1 = min(R, r0 + rows)
+            rd = ref.subset(r0, r1).to_device(dev)
+            parts = [(qry.subset(r0, r1), r0, dict(cfg, symmetric=1))]
+            if r1 < R:
+                parts.append((qry.subset(r1, R), r1, dict(cfg)))
+            for qpart, c0, c in parts:
+                qd = qpart.to_device(dev)
+                bufs = (torch.empty((r1 - r0, qd.n), dtype=torch.float32, device=dev),
+                        torch.empty((r1 - r0, qd.n), dtype=torch.int32, device=dev),
+                        torch.empty((r1 - r0, qd.n), dtype=torch.uint8, device=dev))
+                timer = CudaTimer(stream)
+                timer.start()
+                kernels.cosine_greedy_dense(rd, qd, self.tolerance, self.shift,
+                                            self.match_limit, out=bufs, config=c,
+                                            stream=stream, check_errors=True)
+                timer.stop()
+                self.kernel_time += timer.elapsed_seconds()
+                c1 = c0 + qd.n
+                score[r0:r1, c0:c1] = bufs[0].cpu().numpy()
+                matches[r0:r1, c0:c1] = bufs[1].cpu().numpy()
+                overflow[r0:r1, c0:c1] = bufs[2].cpu().numpy()
+            if r0 > 0:
+                score[r0:r1, :r0] = score[:r0, r0:r1].T
+                matches[r0:r1, :r0] = matches[:r0, r0:r1].T
+                overflow[r0:r1, :r0] = overflow[:r0, r0:r1].T
+        return score, matches, overflow
+
     def pair(self, reference, query) -> np.ndarray:
         result_mat = self.matrix([reference], [query])
         return np.asarray(result_mat.squeeze(), dtype=self.score_datatype)
@@ -191,10 +236,11 @@ class CudaCosineGreedy(BaseSimilarity):
         array_type "numpy": np.recarray [R, Q] with fields score/matches/overflow.
         array_type "sparse": StackedSparseArray(R, Q) holding, under the name
         "sparse", every pair with score >= sparse_threshold.
+        is_symmetric=True (matchms semantics; the reference warns and ignores
+        it, CudaCosineGreedy.py:131-132): R == Q, pairs (i, j) with i <= j are
+        scored as (references[i], queries[j]) and (j, i) gets the same result.
         """
         assert self.kernel is not None, "Kernel isn't compiled - use .compile() first"
-        if is_symmetric:
-            warnings.warn("is_symmetric is ignored here, it has no effect.")
         if array_type == "sparse":
             assert self.sparse_threshold is not None, (
                 "When using array_type `sparse` you have to set `score_threshold`. "
@@ -205,12 +251,15 @@ class CudaCosineGreedy(BaseSimilarity):
 
         ref = self.pack(references)
         qry = self.pack(queries)
+        if is_symmetric and ref.n != qry.n:
+            raise ValueError(f"Found unequal number of spectra {ref.n} and {qry.n} while "
+                             "`is_symmetric` is True.")
         if array_type == "numpy":
-            score, matches, overflow = self._compute(ref, qry)
+            score, matches, overflow = self._compute(ref, qry, symmetric=is_symmetric)
             return np.rec.fromarrays([score, matches, overflow], dtype=self.score_datatype)
-        return self._sparse(ref, qry)
+        return self._sparse(ref, qry, symmetric=is_symmetric)
 
-    def _sparse(self, ref: PackedSpectra, qry: PackedSpectra):
+    def _sparse(self, ref: PackedSpectra, qry: PackedSpectra, symmetric: bool = False):
         import torch
 
         R, Q = ref.n, qry.n
@@ -218,13 +267,15 @@ class CudaCosineGreedy(BaseSimilarity):
         thr = float(self.sparse_threshold)
         if thr <= 0.0 or R == 0 or Q == 0:
             # every pair qualifies (scores are >= 0): dense result, all entries
-            score, matches, overflow = self._compute(ref, qry)
+            score, matches, overflow = self._compute(ref, qry, symmetric=symmetric)
             keep = score >= thr
             r, q = np.nonzero(keep)
             s, m, o = score[r, q], matches[r, q], overflow[r, q]
         else:
             dev = self._torch_device()
             cfg = self._config_for(ref, qry)
+            if symmetric:
+                cfg = dict(cfg, symmetric=1)
             stream = torch.cuda.current_stream(dev)
             timer = CudaTimer(stream)
             timer.start()

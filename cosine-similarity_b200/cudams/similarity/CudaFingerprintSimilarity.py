@@ -55,7 +55,7 @@ class CudaFingerprintSimilarity(BaseSimilarity):
             return float(self.set_empty_scores)
         return 0.0  # reference: the matrix starts as zeros (create_full_matrix)
 
-    def _compute(self, fps_ref, fps_qry) -> np.ndarray:
+    def _compute(self, fps_ref, fps_qry, symmetric: bool = False) -> np.ndarray:
         import torch
 
         dev = _native.require_cuda(self._device_index)
@@ -70,7 +70,7 @@ class CudaFingerprintSimilarity(BaseSimilarity):
             qb = np.zeros((qb.shape[0], n_words), np.uint32)
         t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
         out = kernels.fingerprint_matrix(self.similarity_measure, t(rb), t(rv), t(qb), t(qv),
-                                         n_words, self._fill())
+                                         n_words, self._fill(), symmetric=symmetric)
         return out.cpu().numpy()
 
     def pair(self, reference, query) -> np.ndarray:
@@ -87,7 +87,11 @@ class CudaFingerprintSimilarity(BaseSimilarity):
         is_symmetric: bool = False,
     ):
         """Matrix of fingerprint similarities [R, Q] (float32), or a
-        StackedSparseArray for array_type="sparse"."""
+        StackedSparseArray for array_type="sparse".
+
+        is_symmetric=True (matchms semantics; the reference ignores the flag):
+        R == Q, pairs (i, j) with i <= j are computed and mirrored to (j, i),
+        which halves the popcount work."""
         fps_ref = [s.get("fingerprint") for s in references]
         fps_qry = [s.get("fingerprint") for s in queries]
         n_ref = sum(fp is not None for fp in fps_ref)
@@ -98,7 +102,10 @@ class CudaFingerprintSimilarity(BaseSimilarity):
         )
         if array_type not in ("numpy", "sparse"):
             raise NotImplementedError("Output array type is not yet implemented.")
-        similarity_matrix = self._compute(fps_ref, fps_qry)
+        if is_symmetric and len(references) != len(queries):
+            raise ValueError(f"Found unequal number of spectra {len(references)} and "
+                             f"{len(queries)} while `is_symmetric` is True.")
+        similarity_matrix = self._compute(fps_ref, fps_qry, symmetric=is_symmetric)
         if array_type == "sparse":
             scores_array = StackedSparseArray(len(references), len(queries))
             scores_array.add_dense_matrix(similarity_matrix.astype(self.score_datatype), "")

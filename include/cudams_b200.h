@@ -123,6 +123,14 @@ int cms_cosine_greedy_plain(const float* ref_mz, const double* ref_a, const doub
  *   cand_per_pair  expected candidates per pair (e.g. sampled on the host);
  *                  sizes the first query sub-range of large spectra so the
  *                  join's candidate pool rarely overflows (0: unknown)
+ * One field changes the result rather than the speed:
+ *   symmetric      nonzero: matchms' is_symmetric=True (matchms
+ *                  BaseSimilarity.matrix; accepted but ignored by the
+ *                  reference, CudaCosineGreedy.py:131-132).  Needs
+ *                  n_ref == n_q.  Only the pairs (i, j) with i <= j are
+ *                  computed, as (reference i, query j); the dense output
+ *                  copies each to (j, i), the sparse output emits both
+ *                  (i, j) and (j, i) for i != j.
  */
 typedef struct {
     int32_t tile_spectra;
@@ -131,6 +139,7 @@ typedef struct {
     int32_t mode;
     int32_t pair_threads;
     double cand_per_pair;
+    int32_t symmetric;
 } cms_cosine_config;
 
 /*
@@ -253,6 +262,19 @@ int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a, const do
 int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
                     int64_t n_ref, const uint32_t* q_bits, const uint8_t* q_valid, int64_t n_q,
                     int n_words, float fill, float* out, int64_t ld, void* stream);
+
+/*
+ * cms_fingerprint with matchms' is_symmetric=True (the reference's
+ * CudaFingerprintSimilarity.matrix accepts the flag and ignores it,
+ * CudaFingerprintSimilarity.py:113-119): n references and n queries; only the
+ * pairs (i, j) with i <= j are computed, as (reference i, query j), and
+ * (j, i) receives the same value.  Half of the popcount work of
+ * cms_fingerprint; for one set against itself the result is bit-identical
+ * to it (every measure is symmetric in I, a and b).
+ */
+int cms_fingerprint_symmetric(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
+                              const uint32_t* q_bits, const uint8_t* q_valid, int64_t n,
+                              int n_words, float fill, float* out, int64_t ld, void* stream);
 
 #ifdef __cplusplus
 }

@@ -80,6 +80,25 @@ def cosine_greedy(ref, qry, tolerance: float, shift: float, match_limit: int,
     return score, matches, overflow
 
 
+def cosine_greedy_symmetric(ref, qry, tolerance: float, shift: float, match_limit: int,
+                            key_mode: int = 0, threads: int = 0):
+    """matchms is_symmetric=True (matchms>=0.24 BaseSimilarity.matrix, the
+    pin of requirements.txt:1; the reference accepts and ignores the flag,
+    CudaCosineGreedy.py:131-132): pair (i, j) with i <= j is scored as
+    (references[i], queries[j]) and (j, i) receives the same result."""
+    full = cosine_greedy(ref, qry, tolerance, shift, match_limit, key_mode, threads)
+    n = full[0].shape[0]
+    if full[0].shape[1] != n:
+        raise ValueError("symmetric scoring needs as many queries as references")
+    lower = np.tril_indices(n, -1)
+    out = []
+    for a in full:
+        a = a.copy()
+        a[lower] = a.T[lower]
+        out.append(a)
+    return tuple(out)
+
+
 def cosine_greedy_pairs(ref, qry, pair_r, pair_q, tolerance: float, shift: float,
                         match_limit: int, key_mode: int = 0, threads: int = 0):
     rm, ra, rb, ro = _side(ref)

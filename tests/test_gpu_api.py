@@ -65,11 +65,9 @@ def test_cosine_greedy_matrix(cuda_device, symmetric):
     spectrum_2 = Spectrum(np.array([110, 190, 290.0]), np.array([0.5, 0.2, 1.0]))
     spectrums = [spectrum_1, spectrum_2]
     cosine_greedy = CudaCosineGreedy(batch_size=8)
-    if symmetric:
-        with pytest.warns(UserWarning):
-            scores = cosine_greedy.matrix(spectrums, spectrums, is_symmetric=symmetric)
-    else:
-        scores = cosine_greedy.matrix(spectrums, spectrums, is_symmetric=symmetric)
+    # the reference warns that is_symmetric is ignored (CudaCosineGreedy.py:131-132);
+    # here it is implemented (upper triangle computed, mirrored), so no warning
+    scores = cosine_greedy.matrix(spectrums, spectrums, is_symmetric=symmetric)
     assert scores[0][0][0] == pytest.approx(scores[1][1][0], 0.000001)
     assert scores[0][0]["score"] == pytest.approx(scores[1][1]["score"], 0.000001)
     assert scores[0][1][0] == pytest.approx(scores[1][0][0], 0.000001)

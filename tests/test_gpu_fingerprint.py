@@ -111,3 +111,53 @@ def test_large_symmetric(cuda_device):
     rows = rng.integers(0, 12000, 64)
     want = oracle.fingerprint("jaccard", bits[rows], None, bits, None, bits.shape[1], np.nan)
     _bits_equal(got[rows], want)
+
+
+@pytest.mark.parametrize("n", [301, 320])  # 320: 16-aligned rows (vector mirror)
+@pytest.mark.parametrize("measure", MEASURES)
+def test_symmetric(cuda_device, measure, n):
+    """is_symmetric=True: (i, j), i <= j, computed as (reference i, query j)
+    and mirrored.  For one set against itself this equals the full matrix bit
+    for bit; for two sets the lower triangle is the mirrored upper one."""
+    import torch
+
+    from cudams import kernels, synthetic
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    n_words = 64   # 3 tile rows/columns of 128, ragged edge
+    a = synthetic.fingerprints(n, seed=11)
+    b = synthetic.fingerprints(n, seed=12)
+    va = np.ones(n, np.uint8)
+    vb = np.ones(n, np.uint8)
+    va[7] = 0
+    vb[130] = 0
+    full_aa = oracle.fingerprint(measure, a, va, a, va, n_words, np.nan)
+    got = kernels.fingerprint_matrix(measure, t(a), t(va), t(a), t(va), n_words, np.nan,
+                                     symmetric=True).cpu().numpy()
+    _bits_equal(got, full_aa)
+
+    full_ab = oracle.fingerprint(measure, a, va, b, vb, n_words, -1.0)
+    lower = np.tril_indices(n, -1)
+    want = full_ab.copy()
+    want[lower] = full_ab.T[lower]
+    assert (want != full_ab).any()
+    got = kernels.fingerprint_matrix(measure, t(a), t(va), t(b), t(vb), n_words, -1.0,
+                                     symmetric=True).cpu().numpy()
+    _bits_equal(got, want)
+
+
+def test_symmetric_class_api(cuda_device):
+    from conftest import Spectrum
+    from cudams.similarity import CudaFingerprintSimilarity
+
+    rng = np.random.default_rng(13)
+    fps = [(rng.random(2048) < 0.1).astype(np.uint8) for _ in range(40)]
+    spectra = [Spectrum(np.array([100.0]), np.array([1.0]), {"fingerprint": fp}) for fp in fps]
+    spectra[5] = Spectrum(np.array([100.0]), np.array([1.0]))  # no fingerprint
+    sim = CudaFingerprintSimilarity("jaccard", set_empty_scores=0.5)
+    full = sim.matrix(spectra, spectra)
+    sym = sim.matrix(spectra, spectra, is_symmetric=True)
+    _bits_equal(sym, full)
+    with pytest.raises(ValueError, match="is_symmetric"):
+        sim.matrix(spectra, spectra[:-1], is_symmetric=True)
