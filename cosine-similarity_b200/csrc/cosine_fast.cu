@@ -516,8 +516,8 @@ join_kernel(JoinParams P) {
         const double snA = P.snA[a];
 
         int width = tn;
-        if (P.init_width_scale > 0.f && na > 0)
-            width = max(32, min(tn, (int)(P.init_width_scale / (float)na)));
+        if (P.init_width_scale > 0.f && na > 0)  // multiples of 32 keep row writes aligned
+            width = max(32, min(tn, (int)(P.init_width_scale / (float)na) & ~31));
         // queries of this item: the whole tile, or under `sym` those on or
         // above the diagonal (reference index <= query index)
         int range_lo = 0, q_end = tn;
@@ -660,28 +660,37 @@ join_kernel(JoinParams P) {
 
             if (n > 0) {
                 // ---- counting sort of the pool by query ----
-                // exclusive scan of the per-query counts, in place (words of two)
+                // exclusive scan of the per-query counts, in place (words of
+                // two): each step, lane l takes the uint4 (eight counters) at
+                // word 4 * l of a 128-word stripe, so a step's 32 accesses are
+                // consecutive 16-byte words (no bank conflicts); the stripe's
+                // total carries into the next step
                 const int nw = (rw / 2 + 1 + 3) & ~3;  // whole uint4s (zeroed beyond)
-                const int per = ((nw / 4 + 31) / 32) * 4;
-                const int w0 = min(nw, lane * per), w1 = min(nw, w0 + per);
-                unsigned local = 0;
-                for (int w = w0; w < w1; w += 4) {
-                    const uint4 v = *reinterpret_cast<const uint4*>(cnt + w);
-                    local += (v.x & 0xFFFFu) + (v.x >> 16) + (v.y & 0xFFFFu) + (v.y >> 16) +
-                             (v.z & 0xFFFFu) + (v.z >> 16) + (v.w & 0xFFFFu) + (v.w >> 16);
-                }
-                unsigned incl = local;
+                unsigned carry = 0;
+                for (int w = 4 * lane; w - 4 * lane < nw; w += 128) {
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (w < nw) v = *reinterpret_cast<const uint4*>(cnt + w);
+                    const unsigned c0 = v.x & 0xFFFFu, c1 = v.x >> 16, c2 = v.y & 0xFFFFu,
+                                   c3 = v.y >> 16, c4 = v.z & 0xFFFFu, c5 = v.z >> 16,
+                                   c6 = v.w & 0xFFFFu, c7 = v.w >> 16;
+                    const unsigned local = c0 + c1 + c2 + c3 + c4 + c5 + c6 + c7;
+                    unsigned incl = local;
 #pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const unsigned u = __shfl_up_sync(full, incl, d);
-                    if (lane >= d) incl += u;
-                }
-                unsigned run = incl - local;
-                for (int w = w0; w < w1; ++w) {
-                    const uint32_t v = cnt[w];
-                    const unsigned lo = v & 0xFFFFu;
-                    cnt[w] = run | ((run + lo) << 16);
-                    run += lo + (v >> 16);
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const unsigned u = __shfl_up_sync(full, incl, d);
+                        if (lane >= d) incl += u;
+                    }
+                    unsigned run = carry + incl - local;
+                    uint4 o;
+                    o.x = run | ((run + c0) << 16);
+                    run += c0 + c1;
+                    o.y = run | ((run + c2) << 16);
+                    run += c2 + c3;
+                    o.z = run | ((run + c4) << 16);
+                    run += c4 + c5;
+                    o.w = run | ((run + c6) << 16);
+                    if (w < nw) *reinterpret_cast<uint4*>(cnt + w) = o;
+                    carry += __shfl_sync(full, incl, 31);
                 }
                 __syncwarp();
                 // scatter: the counters become run ends
