@@ -9,12 +9,14 @@ Two decisions matter for cms_cosine_greedy:
     the pool rarely overflows, and large enough that the bucket lookups per
     reference peak are amortised over many queries.
 
-Both follow from the expected number of candidates per pair, which is
-measured here on a seeded sample of pairs with numpy (exact window counts,
-no model of the m/z distribution), bucketed by peak count so that long
-spectra are not under-represented.  Tuned settings can be pinned per
-workload key in an on-disk cache (JSON) by `Tuner.record`, which the
-benchmark's tuning pass fills with measured timings.
+Both follow from the expected number of candidates per pair.  Its mean is
+estimated at the peak level: the probability that a random reference peak
+and a random query peak fall within the window (exact window counts of a
+seeded peak sample against a sorted sample of query peaks, with numpy),
+times the peaks per spectrum of each side.  Sampling whole pairs instead
+gives a noisy mean when peak counts are heavy-tailed; the pair sample is
+kept for the 99th percentile.  Tuned settings can be pinned per workload key
+in an on-disk cache (JSON) by `Tuner.record`.
 """
 from __future__ import annotations
 
@@ -35,7 +37,7 @@ DENSE_CANDIDATES = 48.0  # mean candidates per pair above which mode 2 is used
 
 @dataclass
 class WorkloadStats:
-    cand_per_pair: float      # mean candidates per pair (sampled)
+    cand_per_pair: float      # mean candidates per pair (peak-level estimate)
     cand_per_pair_p99: float  # 99th percentile
     mean_peaks_ref: float
     mean_peaks_qry: float
@@ -61,29 +63,56 @@ def sample_candidates(ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
     return counts
 
 
+def mean_candidates(ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
+                    shift: float = 0.0, n_ref_peaks: int = 20_000, n_qry_peaks: int = 400_000,
+                    seed: int = 0) -> float:
+    """Mean candidates per (reference, query) pair from a peak-level sample:
+    P_ref * P_qry * p / (n_ref * n_qry), p = P(|mz_q + shift - mz_r| <= tol)
+    for a random reference peak and a random query peak."""
+    p_r, p_q = int(ref.mz.shape[0]), int(qry.mz.shape[0])
+    if ref.n == 0 or qry.n == 0 or p_r == 0 or p_q == 0:
+        return 0.0
+    rng = np.random.default_rng(seed)
+    mr = ref.mz if p_r <= n_ref_peaks else ref.mz[rng.integers(0, p_r, n_ref_peaks)]
+    mq = qry.mz if p_q <= n_qry_peaks else qry.mz[rng.integers(0, p_q, n_qry_peaks)]
+    mr = mr.astype(np.float64)
+    mq = np.sort(mq.astype(np.float64) + shift)
+    hits = (np.searchsorted(mq, mr + tolerance, side="right")
+            - np.searchsorted(mq, mr - tolerance, side="left")).sum()
+    p = float(hits) / (float(mr.shape[0]) * float(mq.shape[0]))
+    return p * p_r * p_q / (float(ref.n) * float(qry.n))
+
+
 def workload_stats(ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
                    shift: float = 0.0, n_pairs: int = 512, seed: int = 0) -> WorkloadStats:
     c = sample_candidates(ref, qry, tolerance, shift, n_pairs, seed)
-    return WorkloadStats(float(c.mean()) if c.size else 0.0,
+    return WorkloadStats(mean_candidates(ref, qry, tolerance, shift, seed=seed),
                          float(np.percentile(c, 99)) if c.size else 0.0,
                          float(ref.lengths.mean()) if ref.n else 0.0,
                          float(qry.lengths.mean()) if qry.n else 0.0)
 
 
-# work items (reference spectrum x query tile) wanted per launch: several per
-# resident warp of the join kernel (148 SMs x 32 warps), so that small
-# problems still fill the GPU
-TARGET_ITEMS = 40_000
+# work items (reference spectrum x query tile) wanted per launch: tens per
+# resident warp of the join kernel (148 SMs x 24 warps), so that small
+# problems still fill the GPU and the last items do not leave it idle
+TARGET_ITEMS = 100_000
+# expected candidates per work item: measured on B200 with lognormal spectra
+# (tol 0.01, ~0.1 candidates per pair) the time per pair is flat within 3%
+# between ~100 and ~180 candidates per item from 20k x 20k to 100k x 100k
+# (tiles 1024-1792); below ~75 the per-peak bucket lookups dominate
+CANDIDATES_PER_ITEM = 128.0
+# largest automatic tile: the join's per-warp query counters grow with the
+# tile, and above ~2300 queries three CTAs no longer fit an SM
+MAX_AUTO_TILE = 2048
 
 
 def heuristic_config(stats: WorkloadStats, n_q: int, n_ref: int = 1 << 30) -> dict:
     if stats.cand_per_pair >= DENSE_CANDIDATES:
         return {"mode": 2}
     per_pair = max(stats.cand_per_pair, 1e-4)
-    # measured optimum on B200: ~70 expected candidates per (reference, tile)
-    tile = int(70.0 / per_pair)
+    tile = int(CANDIDATES_PER_ITEM / per_pair)
     tile = min(tile, max(32, (n_ref * n_q) // TARGET_ITEMS))
-    tile = max(32, min(4096, tile))
+    tile = max(32, min(MAX_AUTO_TILE, tile))
     tile = (tile + 31) // 32 * 32
     tile = min(tile, max(32, (n_q + 31) // 32 * 32))
     return {"mode": 1, "tile_spectra": tile, "cand_per_pair": float(stats.cand_per_pair)}
