@@ -998,6 +998,98 @@ struct PairParams {
     int sym;  // only pairs (reference i, query j) with i <= j
 };
 
+// Register-blocked bitonic sort of m = 8 * blockDim.x candidates, descending by
+// (order key, gen), for the pair kernel: each thread holds the 8 consecutive
+// elements 8t..8t+7 in registers.  Exchange distance j < 8: inside the
+// thread; 8 <= j < 256: with lane t ^ (j / 8) of the same warp by shuffle;
+// j >= 256: with thread t ^ (j / 8) of another warp through shared memory
+// (element-major staging, so those accesses have no bank conflicts).  The
+// network and the result are those of the plain shared-memory bitonic sort.
+struct Cand {
+    unsigned long long k;
+    uint32_t g;
+};
+__device__ __forceinline__ bool cand_gt(const Cand& a, const Cand& b) {
+    return a.k > b.k || (a.k == b.k && a.g > b.g);
+}
+// keep the larger of the pair (i, i ^ j) at the lower index when the block
+// of kk elements containing i sorts descending
+template <int J>
+__device__ __forceinline__ void sort8_local(Cand (&c)[8], int base, int kk) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        if (e & J) continue;
+        const int f = e | J;
+        const bool desc = ((base + e) & kk) == 0;
+        const bool gt = cand_gt(c[e], c[f]);
+        if (desc ? !gt : gt) {
+            const Cand t = c[e];
+            c[e] = c[f];
+            c[f] = t;
+        }
+    }
+}
+__device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int base = 8 * tid;
+    const unsigned full = 0xffffffffu;
+    Cand c[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        c[e].k = okey[base + e];
+        c[e].g = cgen[base + e];
+    }
+    for (int kk = 2; kk <= m; kk <<= 1) {
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            if (j >= 8) {
+                const int pt = tid ^ (j >> 3);
+                const bool lower = (base & j) == 0;
+                const bool desc = (base & kk) == 0;  // kk >= 16: the same for all e
+                Cand o[8];
+                if (j >= 256) {
+                    __syncthreads();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        okey[e * nt + tid] = c[e].k;
+                        cgen[e * nt + tid] = c[e].g;
+                    }
+                    __syncthreads();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        o[e].k = okey[e * nt + pt];
+                        o[e].g = cgen[e * nt + pt];
+                    }
+                } else {
+                    const int d = j >> 3;
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        o[e].k = __shfl_xor_sync(full, c[e].k, d);
+                        o[e].g = __shfl_xor_sync(full, c[e].g, d);
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const bool gt = cand_gt(c[e], o[e]);
+                    if ((lower == desc) ? !gt : gt) c[e] = o[e];
+                }
+            } else if (j == 4) {
+                sort8_local<4>(c, base, kk);
+            } else if (j == 2) {
+                sort8_local<2>(c, base, kk);
+            } else {
+                sort8_local<1>(c, base, kk);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        okey[base + e] = c[e].k;
+        cgen[base + e] = c[e].g;
+    }
+    __syncthreads();
+}
+
 template <bool SPARSE>
 __global__ void pair_kernel(PairParams P) {
     if (*P.bad) return;
@@ -1113,7 +1205,11 @@ __global__ void pair_kernel(PairParams P) {
             for (int i = tid; i < (nr + 31) / 32; i += blockDim.x) used_r[i] = 0u;
             for (int i = tid; i < (nq + 31) / 32; i += blockDim.x) used_q[i] = 0u;
             __syncthreads();
-            // bitonic sort, descending by (okey, gen)
+            // bitonic sort, descending by (okey, gen): in registers when the
+            // block holds exactly eight candidates a thread, else in shared memory
+            if (m == 8 * (int)blockDim.x) {
+                sort8_block(okey, cgen, m);
+            } else
             for (int k = 2; k <= m; k <<= 1) {
                 for (int j = k >> 1; j > 0; j >>= 1) {
                     for (int i = tid; i < m; i += blockDim.x) {
@@ -1244,12 +1340,16 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
     p.nb = (cfg && cfg->n_buckets > 0) ? next_pow2(cfg->n_buckets)
                                        : next_pow2((long long)std::max(1024.0, avg_tile_peaks));
     p.nb = std::min(p.nb, 1 << 22);
-    p.pair_threads = (cfg && cfg->pair_threads > 0) ? cfg->pair_threads : 128;
+    p.cap = next_pow2(std::max(2, args.match_limit));
+    // whole-matrix pair kernel (mode 2): pairs usually fill match_limit, and
+    // eight candidates a thread sort in registers; spilled pairs vary in size
+    p.pair_threads = (cfg && cfg->pair_threads > 0)
+                         ? cfg->pair_threads
+                         : (p.mode == 2 ? std::max(64, std::min(512, p.cap / 8)) : 128);
     if (p.pair_threads < 64 || p.pair_threads > 512 || p.pair_threads % 32) {
         set_error("cms_cosine_greedy: pair_threads must be a multiple of 32 in [64, 512]");
         return CMS_ERR_INVALID;
     }
-    p.cap = next_pow2(std::max(2, args.match_limit));
     const long long pairs = (long long)args.ref.n * (long long)args.qry.n;
     long long sc = std::max<long long>(1 << 20, pairs / 64);
     sc = std::min<long long>(sc, std::min<long long>(pairs, 1LL << 28));

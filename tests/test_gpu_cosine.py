@@ -76,6 +76,33 @@ def test_clustered_overflow(cuda_device):
     assert_same(gpu_plain(ref, qry, p), want, "plain")
 
 
+@pytest.mark.parametrize("ml, threads", [(512, 64), (1024, 128), (2048, 256), (4096, 512),
+                                         (1000, 128), (700, 64)])
+def test_pair_kernel_register_sort(cuda_device, ml, threads):
+    """The pair kernel sorts in registers when a pair's padded candidate count
+    is eight per thread (pairs that fill match_limit with threads = cap / 8),
+    and in shared memory otherwise; both bit-exact.  Clustered spectra fill any
+    of these limits; a few empty and short spectra give small pairs too."""
+    from cudams import synthetic
+    from cudams.packing import PackedSpectra
+
+    ref = synthetic.clustered_spectra(18, seed=7, min_peaks=600, max_peaks=1500)
+    qry = synthetic.clustered_spectra(14, seed=8, min_peaks=600, max_peaks=1500)
+    # append a 3-peak and an empty query so that some pairs are tiny
+    mz = np.concatenate([qry.mz, np.array([100.0, 200.0, 300.0], np.float32)])
+    b = np.concatenate([qry.b, np.array([1.0, 0.5, 0.25])])
+    a = None if qry.a is None else np.concatenate([qry.a, np.ones(3)])
+    off = np.concatenate([qry.offsets, [qry.offsets[-1] + 3, qry.offsets[-1] + 3]])
+    qry2 = PackedSpectra(mz, a, b, off.astype(np.int64), qry.mz_power, qry.intensity_power,
+                         qry.n_max_peaks)
+    p = P(0.05, ml, 2048)
+    want = oracle.cosine_greedy(ref, qry2, 0.05, 0.0, ml)
+    assert want[2].mean() > 0.5
+    assert_same(gpu_dense(ref, qry2, p, {"mode": 2, "pair_threads": threads}), want,
+                f"ml {ml} threads {threads}")
+    assert_same(gpu_dense(ref, qry2, p, {"mode": 2}), want, f"ml {ml} auto threads")
+
+
 def test_self_similarity_spills(cuda_device):
     """Identical sets: diagonal pairs have one candidate per peak (long runs ->
     pair kernel), off-diagonal pairs few; both paths must agree."""
