@@ -1230,39 +1230,54 @@ __global__ void pair_kernel(PairParams P) {
                     __syncthreads();
                 }
             }
-            // greedy by warp 0: chunks of 32 in order, leaders in lane order
+            // greedy by warp 0 over chunks of 32 sorted candidates.  Within a
+            // chunk a live candidate is accepted iff no earlier accepted one
+            // shares its reference or query peak: conflict masks come from
+            // __match_any_sync, and lanes decide in rounds, each lane as soon as
+            // every earlier conflicting lane has decided (the lowest undecided
+            // lane always can, so this ends; usually after one or two rounds).
+            // Accepted keys are summed in sorted order, as the sequential greedy.
             if (wid == 0) {
+                const unsigned below = (1u << lane) - 1u;
                 for (int c = 0; c < n; c += 32) {
                     const int i = c + lane;
                     uint32_t g = 0;
-                    double kk = 0.0;
                     bool alive = false;
                     if (i < n) {
                         g = cgen[i];
-                        kk = key_from_order(okey[i]);
                         const int p1 = g >> 16, p2 = g & 0xFFFF;
                         alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
                                 !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
                     }
-                    unsigned bal = __ballot_sync(full, alive);
-                    while (bal) {
-                        const int leader = __ffs(bal) - 1;
-                        const uint32_t lg = __shfl_sync(full, g, leader);
-                        const double lk = __shfl_sync(full, kk, leader);
-                        if (lane == 0) {
-                            score = __dadd_rn(score, lk);
-                            ++matches;
+                    const unsigned live = __ballot_sync(full, alive);
+                    if (live == 0u) continue;
+                    // dead lanes get values no peak index takes, so they match
+                    // only themselves
+                    const unsigned m1 = __match_any_sync(full, alive ? (g >> 16) : 0x10000u + lane);
+                    const unsigned m2 =
+                        __match_any_sync(full, alive ? (g & 0xFFFFu) : 0x10000u + lane);
+                    const unsigned earlier = (m1 | m2) & live & below;
+                    unsigned dec = ~live, acc = 0u;
+                    while (dec != full) {
+                        bool my_dec = (dec >> lane) & 1u, my_acc = (acc >> lane) & 1u;
+                        if (!my_dec && (earlier & ~dec) == 0u) {
+                            my_dec = true;
+                            my_acc = (earlier & acc) == 0u;
                         }
-                        if (lane == leader) {
-                            const int p1 = lg >> 16, p2 = lg & 0xFFFF;
-                            used_r[p1 >> 5] |= 1u << (p1 & 31);
-                            used_q[p2 >> 5] |= 1u << (p2 & 31);
-                            alive = false;
-                        }
-                        if (alive && (((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu))))
-                            alive = false;
-                        bal = __ballot_sync(full, alive);
+                        dec = __ballot_sync(full, my_dec);
+                        acc = __ballot_sync(full, my_acc);
                     }
+                    if ((acc >> lane) & 1u) {
+                        const int p1 = g >> 16, p2 = g & 0xFFFF;
+                        atomicOr(&used_r[p1 >> 5], 1u << (p1 & 31));
+                        atomicOr(&used_q[p2 >> 5], 1u << (p2 & 31));
+                    }
+                    const double kk = (i < n) ? key_from_order(okey[i]) : 0.0;
+                    for (unsigned a = acc; a; a &= a - 1u) {
+                        const double k = __shfl_sync(full, kk, __ffs(a) - 1);
+                        score = __dadd_rn(score, k);
+                    }
+                    matches += __popc(acc);
                     __syncwarp();
                 }
             }
