@@ -353,17 +353,6 @@ struct Pool {
         else
             gperm[pos - kPool] = (uint16_t)slot;
     }
-    // a run's result, packed into the key slot of its first candidate
-    __device__ __forceinline__ void set_result(int i, int2 r) const {
-        if (i < kPool)
-            reinterpret_cast<int2*>(skey)[i] = r;
-        else
-            reinterpret_cast<int2*>(gkey)[i - kPool] = r;
-    }
-    __device__ __forceinline__ int2 result(int i) const {
-        return i < kPool ? reinterpret_cast<const int2*>(skey)[i]
-                         : reinterpret_cast<const int2*>(gkey)[i - kPool];
-    }
 };
 
 // Per-warp shared-memory slice (offsets in bytes; the count array's length
@@ -503,10 +492,15 @@ join_kernel(JoinParams P) {
         if (lane == 0) base = atomicAdd(P.work, (unsigned long long)kFetch);
         base = __shfl_sync(full, base, 0);
         if ((int64_t)base >= n_items) break;
-        for (int f = 0; f < kFetch && (int64_t)(base + f) < n_items; ++f) {
-        const int64_t item = (int64_t)base + f;
-        const int t = (int)(item / nA);
-        const int a = P.a_order[item % nA];
+        // item = t * nA + ai: one division per fetch, then step ai
+        int64_t tt = (int64_t)base / nA, ai = (int64_t)base - tt * nA;
+        for (int f = 0; f < kFetch && (int64_t)(base + f) < n_items; ++f, ++ai) {
+        while (ai >= nA) {
+            ai -= nA;
+            ++tt;
+        }
+        const int t = (int)tt;
+        const int a = P.a_order[ai];
         const int64_t a0 = P.A.off[a];
         const int na = (int)(P.A.off[a + 1] - a0);
         const int b_begin = t * P.g.tile;
@@ -514,6 +508,12 @@ join_kernel(JoinParams P) {
         const int64_t tbase = P.B.off[b_begin];
         const uint32_t* T = tab + (int64_t)t * (P.g.nb + 1);
         const double snA = P.snA[a];
+        // a resolved run's result, stored straight into the dense output
+        auto put_dense = [&](int bq, float sc, int mt) {
+            const int64_t o = (int64_t)(A_IS_REF ? a : bq) * P.dense.ld + (A_IS_REF ? bq : a);
+            __stcs(&P.dense.score[o], sc);
+            __stcs(&P.dense.matches[o], mt);
+        };
 
         int width = tn;
         if (P.init_width_scale > 0.f && na > 0)  // multiples of 32 keep row writes aligned
@@ -772,7 +772,7 @@ join_kernel(JoinParams P) {
                             if (sc >= P.sparse.threshold)
                                 emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
                         } else {
-                            pool.set_result(sl, make_int2(__float_as_int(sc), mt));
+                            put_dense(bq, sc, mt);
                         }
                     }
                 }
@@ -829,7 +829,7 @@ join_kernel(JoinParams P) {
                             if (sc >= P.sparse.threshold)
                                 emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
                         } else {
-                            pool.set_result(pool.perm(i0), make_int2(__float_as_int(sc), mt));
+                            put_dense(bq, sc, mt);
                         }
                     }
                 }
@@ -899,70 +899,64 @@ join_kernel(JoinParams P) {
                         if (mt > 0 && sc >= P.sparse.threshold)
                             emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
                     } else {
-                        pool.set_result(pool.perm(i), make_int2(__float_as_int(sc), mt));
+                        put_dense(bq, sc, mt);
                     }
                 }
             }
             __syncwarp();
             flush_long();
-            // ---- write the results (sparse hits were emitted above) ----
+            // ---- zeros for the queries without a candidate ----
             if (!SPARSE) {
-                // dense row segment out[a, b_begin + range_lo ...): every query
-                // of the range, zeros where there is no candidate; 4 queries per
-                // lane with 16-byte streaming stores when aligned
+                // dense row segment out[a, b_begin + range_lo ...): the runs'
+                // results were stored as they were resolved; every other query
+                // of the range gets score 0, matches 0, and every query overflow
+                // 0 (a spilled pair's is rewritten by the pair kernel).  Four
+                // queries per lane, 16-byte streaming stores when aligned.
                 const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
-                auto result_of = [&](int qr, float& sc, int& mt) {
-                    sc = 0.f;
-                    mt = 0;
-                    if (n > 0) {
-                        const int e = (int)cnt_get(cnt, qr);
-                        const int s = qr > 0 ? (int)cnt_get(cnt, qr - 1) : 0;
-                        if (e > s) {
-                            const int2 r = pool.result(pool.perm(s));
-                            sc = __int_as_float(r.x);
-                            mt = r.y;
-                        }
-                    }
-                };
                 int qv = 0;
                 if ((row & 3) == 0 && (P.dense.ld & 3) == 0) {
                     for (; qv + 128 <= rw; qv += 128) {
                         const int q0 = qv + 4 * lane;
-                        float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                        int4 m4 = make_int4(0, 0, 0, 0);
+                        // run ends of queries q0..q0+3 and of q0-1 (start of q0)
+                        unsigned e0 = 0, e1 = 0, e2 = 0, e3 = 0, sp = 0;
                         if (n > 0) {
-                            // ends of queries q0..q0+3 and of q0-1 (= start of q0)
                             const uint2 w = *reinterpret_cast<const uint2*>(cnt + (q0 >> 1));
-                            const unsigned e0 = w.x & 0xFFFFu, e1 = w.x >> 16;
-                            const unsigned e2 = w.y & 0xFFFFu, e3 = w.y >> 16;
-                            const unsigned sp = q0 > 0 ? (cnt[(q0 >> 1) - 1] >> 16) : 0u;
-                            if (e3 > sp) {
-                                auto fetch = [&](unsigned st, unsigned en, float& sc, int& mt) {
-                                    if (en > st) {
-                                        const int2 r = pool.result(pool.perm((int)st));
-                                        sc = __int_as_float(r.x);
-                                        mt = r.y;
-                                    }
-                                };
-                                fetch(sp, e0, s4.x, m4.x);
-                                fetch(e0, e1, s4.y, m4.y);
-                                fetch(e1, e2, s4.z, m4.z);
-                                fetch(e2, e3, s4.w, m4.w);
-                            }
+                            e0 = w.x & 0xFFFFu;
+                            e1 = w.x >> 16;
+                            e2 = w.y & 0xFFFFu;
+                            e3 = w.y >> 16;
+                            sp = q0 > 0 ? (cnt[(q0 >> 1) - 1] >> 16) : 0u;
                         }
-                        __stcs(reinterpret_cast<float4*>(P.dense.score + row + q0), s4);
-                        __stcs(reinterpret_cast<int4*>(P.dense.matches + row + q0), m4);
                         __stcs(reinterpret_cast<uchar4*>(P.dense.overflow + row + q0),
                                make_uchar4(0, 0, 0, 0));
+                        if (e3 == sp) {
+                            __stcs(reinterpret_cast<float4*>(P.dense.score + row + q0),
+                                   make_float4(0.f, 0.f, 0.f, 0.f));
+                            __stcs(reinterpret_cast<int4*>(P.dense.matches + row + q0),
+                                   make_int4(0, 0, 0, 0));
+                        } else {
+                            const unsigned st[4] = {sp, e0, e1, e2}, en[4] = {e0, e1, e2, e3};
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                if (en[k] == st[k]) {
+                                    __stcs(&P.dense.score[row + q0 + k], 0.f);
+                                    __stcs(&P.dense.matches[row + q0 + k], 0);
+                                }
+                            }
+                        }
                     }
                 }
                 for (int qr = qv + lane; qr < rw; qr += 32) {
-                    float sc;
-                    int mt;
-                    result_of(qr, sc, mt);
-                    __stcs(&P.dense.score[row + qr], sc);
-                    __stcs(&P.dense.matches[row + qr], mt);
+                    bool empty = true;
+                    if (n > 0) {
+                        const unsigned e = cnt_get(cnt, qr);
+                        empty = e == (qr > 0 ? cnt_get(cnt, qr - 1) : 0u);
+                    }
                     __stcs(&P.dense.overflow[row + qr], (unsigned char)0);
+                    if (empty) {
+                        __stcs(&P.dense.score[row + qr], 0.f);
+                        __stcs(&P.dense.matches[row + qr], 0);
+                    }
                 }
             }
             __syncwarp();
