@@ -72,21 +72,26 @@ class PackedSpectra:
                    + (self.a.nbytes if self.a is not None else 0))
 
     def to_device(self, device, non_blocking: bool = False):
-        """DeviceSpectra on `device` (cached per device)."""
+        """DeviceSpectra on `device` (cached per device).  Large arrays go through
+        the pinned staging ring (`cudams.staging`): the copies are enqueued on
+        the current stream, so work on that stream sees the data; use another
+        stream only after synchronising (or pass non_blocking=False, the
+        default, which waits for the copies)."""
         import torch
+
+        from . import staging
 
         key = str(device)
         if key not in self._device:
             def up(x):
                 if x is None:
                     return None
-                t = torch.from_numpy(np.ascontiguousarray(x))
-                if non_blocking:
-                    t = t.pin_memory()
-                return t.to(device, non_blocking=non_blocking)
+                return staging.upload(np.ascontiguousarray(x), device)
 
             self._device[key] = DeviceSpectra(up(self.mz), up(self.a), up(self.b),
                                               up(self.offsets), self.n, self.n_peaks)
+            if not non_blocking:
+                torch.cuda.current_stream(device).synchronize()
         return self._device[key]
 
     def truncate(self, n_max_peaks: Optional[int]) -> "PackedSpectra":

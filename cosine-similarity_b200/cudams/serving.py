@@ -173,16 +173,16 @@ class SpectrumLibrary:
             pass
 
 
-def _upload(p: PackedSpectra, device):
-    """DeviceSpectra of `p` on the current stream (pinned staging, async copy)."""
-    import torch
-
+def _upload(p: PackedSpectra, device, slot: int = 0):
+    """DeviceSpectra of `p`, copied on the current stream: small arrays from
+    pageable memory, large ones through the slot's pinned staging ring."""
+    from . import staging
     from .packing import DeviceSpectra
 
     def up(x):
         if x is None:
             return None
-        return torch.from_numpy(np.ascontiguousarray(x)).pin_memory().to(device, non_blocking=True)
+        return staging.upload(np.ascontiguousarray(x), device, slot=slot)
 
     return DeviceSpectra(up(p.mz), up(p.a), up(p.b), up(p.offsets), p.n, p.n_peaks)
 
