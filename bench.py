@@ -59,7 +59,7 @@ JOIN_TRAFFIC_BYTES_PER_PAIR = 9.88
 def parse():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--spectra", dest="n", type=int, default=100_000, help="spectra per side (default 100k)")
@@ -122,9 +122,12 @@ def make_data(args, rank):
 
 # ----------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """nvidia-smi clock/throttle samples (every 50 ms, timestamped).  Started
+    before the warm-up so that it is sampling when the timed region begins;
+    `mark_start` / `mark_end` bracket the timed region and the summary keeps
+    the samples taken inside it."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -132,12 +135,19 @@ class ClockSampler:
         self.idx = gpu_index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
@@ -147,7 +157,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -160,16 +170,22 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if self.t0 is not None and self.t1 is not None:
+            # samples read inside the timed region (a sample line is read within
+            # a few ms of being taken)
+            inside = [x for x in lines if self.t0 <= x[0] <= self.t1]
+            lines = inside or lines
+        for _, ln in lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
+                sm.append(float(parts[2]))
+                mx = max(mx, float(parts[3]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for n, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
@@ -282,22 +298,28 @@ def run_ours(args, world, rank, local):
             kernels.cosine_greedy_dense(s, qd, TOL, 0.0, MATCH_LIMIT, out=o, config=cfg,
                                         stream=stream)
 
+    clocks = ClockSampler(dev.index).__enter__()
     for _ in range(args.warmup):
         step()
     bits = ctx.take_device_error(_native.stream_handle(stream))
     if bits:
+        clocks.__exit__()
         raise RuntimeError(f"device error word {bits} during warm-up")
     ctx.profile_read(reset=True)
     ctx.profile_enable(True)
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev.index) as clocks:
+    try:
+        clocks.mark_start()
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
+        clocks.mark_end()
+    finally:
+        clocks.__exit__()
     barrier(world)
     ms = e0.elapsed_time(e1)
     stage_ms, stage_n = ctx.profile_read(reset=True)
