@@ -505,12 +505,26 @@ def other_workloads(dev, args):
     u_q = synthetic.uniform_spectra(1024, seed=args.seed + 2).to_device(dev)
     u_cfg = autotune.choose_config(synthetic.uniform_spectra(1024, seed=args.seed + 1),
                                    synthetic.uniform_spectra(1024, seed=args.seed + 2), 0.1)
-    ms_t = _time_ms(lambda: kernels.cosine_greedy_dense(u_r, u_q, 0.1, 0.0, 2048, config=u_cfg))
+    u_out = tuple(torch.empty((1024, 1024), dtype=t, device=dev)
+                  for t in (torch.float32, torch.int32, torch.uint8))
+    ms_t = _time_ms(lambda: kernels.cosine_greedy_dense(u_r, u_q, 0.1, 0.0, 2048, out=u_out,
+                                                        config=u_cfg), reps=20)
+    # the same call replayed from a captured CUDA graph (cms_graph_enable)
+    from cudams import _native as _nat
+
+    gctx = _nat.context(dev.index)
+    gctx.graph_enable(True)
+    try:
+        ms_g = _time_ms(lambda: kernels.cosine_greedy_dense(u_r, u_q, 0.1, 0.0, 2048, out=u_out,
+                                                            config=u_cfg), reps=20)
+    finally:
+        gctx.graph_enable(False)
     ms_p = _time_ms(lambda: kernels.cosine_greedy_plain(u_r, u_q, 0.1, 0.0, 2048, 1024))
     res["uniform_1k"] = {"workload": "1024 x 1024, peaks U{10..200}, tol 0.1, match_limit 2048",
                          "tiled_pairs_per_s": 1024 * 1024 / (ms_t / 1e3),
+                         "tiled_graph_pairs_per_s": 1024 * 1024 / (ms_g / 1e3),
                          "plain_pairs_per_s": 1024 * 1024 / (ms_p / 1e3), "tiled_ms": ms_t,
-                         "tuning": u_cfg}
+                         "tiled_graph_ms": ms_g, "tuning": u_cfg}
 
     # overflow stress: clustered dense spectra, 20k x 20k, nearly every pair overflows
     c_r = synthetic.clustered_spectra(20_000, seed=args.seed + 3)

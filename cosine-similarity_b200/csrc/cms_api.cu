@@ -23,10 +23,17 @@ int cuda_fail(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? CMS_ERR_NOMEM : CMS_ERR_CUDA;
 }
 
+void graph_cache_clear(cms_ctx* ctx) {
+    for (auto& g : ctx->graph_cache)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    ctx->graph_cache.clear();
+}
+
 int arena_reserve(cms_ctx* ctx, Arena& a, size_t bytes, cudaStream_t s) {
     if (bytes <= a.bytes) return CMS_OK;
     // Growing: wait for work that may still use the old block, then replace it.
     if (a.ptr) {
+        graph_cache_clear(ctx);
         CMS_CUDA_TRY(cudaStreamSynchronize(s));
         CMS_CUDA_TRY(cudaFree(a.ptr));
         a.ptr = nullptr;
@@ -83,7 +90,7 @@ static cudaEvent_t pool_event(cms_ctx* ctx) {
 StageScope::StageScope(cms_ctx* ctx, int stage, int n, cudaStream_t s)
     : ctx_(ctx), stage_(stage), s_(s) {
     ctx->launches[stage] += n;
-    if (!ctx->profile) return;
+    if (!ctx->profile || ctx->capturing) return;
     cudaEvent_t start = pool_event(ctx);
     stop_ = pool_event(ctx);
     if (!start || !stop_) {
@@ -108,6 +115,20 @@ int cms_profile_enable(cms_ctx* ctx, int enable) {
         return CMS_ERR_INVALID;
     }
     ctx->profile = enable != 0;
+    return CMS_OK;
+}
+
+int cms_graph_enable(cms_ctx* ctx, int enable) {
+    if (!ctx) {
+        cms::set_error("cms_graph_enable: null context");
+        return CMS_ERR_INVALID;
+    }
+    ctx->graphs = enable != 0;
+    if (!ctx->graphs) {
+        cudaSetDevice(ctx->device);
+        cudaDeviceSynchronize();
+        cms::graph_cache_clear(ctx);
+    }
     return CMS_OK;
 }
 
@@ -182,6 +203,8 @@ int cms_destroy(cms_ctx* ctx) {
     if (!ctx) return CMS_OK;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    cms::graph_cache_clear(ctx);
+    if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
     if (ctx->scratch.ptr) cudaFree(ctx->scratch.ptr);
     for (auto& ev : ctx->events) {
         cudaEventDestroy(ev.second.first);

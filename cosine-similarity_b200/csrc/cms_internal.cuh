@@ -76,6 +76,15 @@ struct Arena {
 
 }  // namespace cms
 
+// A captured call: the key is every argument the launch sequence bakes in
+// (pointers, sizes, parameters, stream, scratch arena), so a replay is valid
+// exactly when a later call has the same key.
+struct cms_graph_entry {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches[CMS_PROFILE_STAGES] = {0, 0, 0, 0, 0};
+};
+
 struct cms_ctx {
     int device = 0;
     int sm_count = 0;
@@ -87,12 +96,23 @@ struct cms_ctx {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
     std::vector<cudaEvent_t> event_pool;
     int64_t launches[CMS_PROFILE_STAGES] = {0, 0, 0, 0, 0};
+    // CUDA graphs (cms_graph_enable): most recently used first
+    bool graphs = false;
+    bool capturing = false;
+    std::vector<cms_graph_entry> graph_cache;
+    // graphs are captured on this stream (capture is not allowed on the legacy
+    // default stream) and launched on the caller's
+    cudaStream_t capture_stream = nullptr;
 };
 
 namespace cms {
 
 // Ensure the arena holds at least `bytes`; returns CMS_OK or an error code.
+// Growing the arena drops the context's captured graphs (they hold its address).
 int arena_reserve(cms_ctx* ctx, Arena& a, size_t bytes, cudaStream_t s);
+
+// Destroy every captured graph of the context.
+void graph_cache_clear(cms_ctx* ctx);
 
 // Bump allocator over an arena region (256-byte aligned slices).
 struct Bump {

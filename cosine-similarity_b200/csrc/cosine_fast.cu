@@ -36,7 +36,9 @@
 //                        used-peak bitmasks.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "cms_internal.cuh"
 
@@ -1312,6 +1314,8 @@ struct Plan {
     int pair_threads;
     int cap;
     unsigned int spill_cap;
+    int sym;               // cms_cosine_config.symmetric
+    double cand_per_pair;  // cms_cosine_config.cand_per_pair (0: unknown)
 };
 
 int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse, Plan& p) {
@@ -1390,12 +1394,19 @@ int launch_join(cms_ctx* ctx, const JoinParams& jp, size_t smem, size_t gpool_wa
     return CMS_OK;
 }
 
+int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
+                   const SparseOut* sparse, const Plan& p, cudaStream_t s);
+int run_cosine_graph(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
+                     const SparseOut* sparse, const Plan& p, cudaStream_t s);
+
 int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
                const SparseOut* sparse, const cms_cosine_config* cfg, cudaStream_t s) {
     Plan p;
     int rc = make_plan(args, cfg, sparse != nullptr, p);
     if (rc) return rc;
     const int sym = (cfg && cfg->symmetric) ? 1 : 0;
+    p.sym = sym;
+    p.cand_per_pair = (cfg && cfg->cand_per_pair > 0.0) ? cfg->cand_per_pair : 0.0;
     if (sym && args.ref.n != args.qry.n) {
         set_error("cms_cosine_greedy: symmetric needs as many queries as references "
                   "(%lld != %lld)", (long long)args.ref.n, (long long)args.qry.n);
@@ -1428,6 +1439,20 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     need += 4096;
     rc = arena_reserve(ctx, ctx->scratch, need, s);
     if (rc) return rc;
+    if (!ctx->graphs) return enqueue_cosine(ctx, args, dense, sparse, p, s);
+    return run_cosine_graph(ctx, args, dense, sparse, p, s);
+}
+
+// The launch sequence of one call, into scratch already reserved for plan p
+// (no allocation or synchronisation inside, so that it can be captured).
+int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
+                   const SparseOut* sparse, const Plan& p, cudaStream_t s) {
+    int rc = CMS_OK;
+    const int sym = p.sym;
+    const size_t pair_smem = (size_t)p.cap * 12 + 2 * 2048 * 4;
+    const int64_t nR = args.ref.n, nQ = args.qry.n;
+    const size_t gpool_warps = (size_t)ctx->sm_count * 64;
+    const size_t gpool_bytes = gpool_warps * (size_t)kGPool * 16;
     Bump bp{(char*)ctx->scratch.ptr, 0, ctx->scratch.bytes};
     uint64_t* small = bp.take<uint64_t>(64);
     uint32_t* bad = reinterpret_cast<uint32_t*>(small);            // word 0
@@ -1543,10 +1568,10 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.shift = args.shift;
     jp.match_limit = args.match_limit;
     jp.init_width_scale = 0.f;
-    if (cfg && cfg->cand_per_pair > 0.0 && args.ref.n > 0) {
+    if (p.cand_per_pair > 0.0 && args.ref.n > 0) {
         // expected candidates of (A spectrum with n peaks, w queries) ~ n*w*lambda
         const double mean_na = (double)args.ref.n_peaks / (double)args.ref.n;
-        const double lambda = cfg->cand_per_pair / std::max(1.0, mean_na);
+        const double lambda = p.cand_per_pair / std::max(1.0, mean_na);
         jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
     }
     jp.warp_smem_bytes = warp_slice_bytes(p.tile);
@@ -1582,6 +1607,110 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         CMS_CUDA_TRY(cudaGetLastError());
     }
     return mirror();
+}
+
+// Graph path of run_cosine: replay a captured launch sequence whose key (every
+// value the sequence bakes in) equals this call's, else capture it on the
+// context's capture stream, instantiate and keep it (most recent first, at
+// most kGraphCache per context); graphs are launched on the caller's stream.
+constexpr size_t kGraphCache = 8;
+int run_cosine_graph(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
+                     const SparseOut* sparse, const Plan& p, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CMS_CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone)  // the caller is capturing: just enqueue
+        return enqueue_cosine(ctx, args, dense, sparse, p, s);
+    std::vector<uint64_t> key;
+    key.reserve(48);
+    auto put = [&](auto v) {
+        static_assert(sizeof(v) <= sizeof(uint64_t), "key field too wide");
+        uint64_t u = 0;
+        std::memcpy(&u, &v, sizeof(v));
+        key.push_back(u);
+    };
+    auto put_set = [&](const SpecSet& x) {
+        put((uintptr_t)x.mz);
+        put((uintptr_t)x.a);
+        put((uintptr_t)x.b);
+        put((uintptr_t)x.off);
+        put(x.n);
+        put(x.n_peaks);
+    };
+    put_set(args.ref);
+    put_set(args.qry);
+    put(args.tol);
+    put(args.shift);
+    put(args.match_limit);
+    put((int)(dense != nullptr));
+    if (dense) {
+        put((uintptr_t)dense->score);
+        put((uintptr_t)dense->matches);
+        put((uintptr_t)dense->overflow);
+        put(dense->ld);
+    }
+    put((int)(sparse != nullptr));
+    if (sparse) {
+        put((uintptr_t)sparse->r);
+        put((uintptr_t)sparse->q);
+        put((uintptr_t)sparse->score);
+        put((uintptr_t)sparse->matches);
+        put((uintptr_t)sparse->overflow);
+        put((uintptr_t)sparse->count);
+        put(sparse->capacity);
+        put(sparse->threshold);
+        put(sparse->mirror);
+    }
+    put(p.mode);
+    put(p.tile);
+    put(p.nb);
+    put(p.width);
+    put(p.pair_threads);
+    put(p.cap);
+    put(p.spill_cap);
+    put(p.sym);
+    put(p.cand_per_pair);
+    put((uintptr_t)ctx->scratch.ptr);
+    put(ctx->scratch.bytes);
+
+    auto& cache = ctx->graph_cache;
+    for (size_t i = 0; i < cache.size(); ++i) {
+        if (cache[i].key != key) continue;
+        if (i) std::rotate(cache.begin(), cache.begin() + i, cache.begin() + i + 1);
+        for (int k = 0; k < CMS_PROFILE_STAGES; ++k) ctx->launches[k] += cache[0].launches[k];
+        CMS_CUDA_TRY(cudaGraphLaunch(cache[0].exec, s));
+        return CMS_OK;
+    }
+
+    if (!ctx->capture_stream)
+        CMS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs_stream = ctx->capture_stream;
+    int64_t before[CMS_PROFILE_STAGES];
+    std::memcpy(before, ctx->launches, sizeof(before));
+    CMS_CUDA_TRY(cudaStreamBeginCapture(cs_stream, cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    const int rc = enqueue_cosine(ctx, args, dense, sparse, p, cs_stream);
+    ctx->capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cs_stream, &g);
+    if (rc != CMS_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        if (rc != CMS_OK) return rc;
+        return cuda_fail(e, "cudaStreamEndCapture");
+    }
+    cms_graph_entry entry;
+    entry.key = std::move(key);
+    const cudaError_t ei = cudaGraphInstantiate(&entry.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+    for (int k = 0; k < CMS_PROFILE_STAGES; ++k) entry.launches[k] = ctx->launches[k] - before[k];
+    if (cache.size() >= kGraphCache) {
+        cudaGraphExecDestroy(cache.back().exec);
+        cache.pop_back();
+    }
+    cache.insert(cache.begin(), std::move(entry));
+    CMS_CUDA_TRY(cudaGraphLaunch(cache[0].exec, s));
+    return CMS_OK;
 }
 
 bool check_common(const CosineArgs& a, const char* who) {

@@ -67,6 +67,7 @@ SIGNATURES = {
         _p, _p, _p, _p, _p, c_int64, _p, _p]),
     "cms_library_destroy": (c_int, [_p]),
     "cms_profile_enable": (c_int, [_p, c_int]),
+    "cms_graph_enable": (c_int, [_p, c_int]),
     "cms_profile_read": (c_int, [_p, _p, _p, c_int]),
     "cms_fingerprint": (c_int, [
         c_int, _p, _p, c_int64, _p, _p, c_int64, c_int, c_float, _p, c_int64, _p]),
@@ -147,6 +148,11 @@ class Context:
         check(load().cms_take_device_error(self.handle, ctypes.byref(bits), stream),
               "cms_take_device_error")
         return int(bits.value)
+
+    def graph_enable(self, on: bool = True) -> None:
+        """Capture repeated identical cms_cosine_greedy(_sparse) calls of this
+        context into CUDA graphs and replay them (cms_graph_enable)."""
+        check(load().cms_graph_enable(self.handle, 1 if on else 0), "cms_graph_enable")
 
     def profile_enable(self, on: bool = True) -> None:
         check(load().cms_profile_enable(self.handle, 1 if on else 0), "cms_profile_enable")

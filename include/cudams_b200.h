@@ -81,6 +81,19 @@ int cms_destroy(cms_ctx* ctx);
 int cms_take_device_error(cms_ctx* ctx, uint32_t* bits, void* stream);
 
 /*
+ * CUDA graphs for repeated calls (no reference counterpart; the reference
+ * relaunches its Numba kernel per batch pair).  When enabled, cms_cosine_greedy
+ * and cms_cosine_greedy_sparse capture their whole launch sequence (validation,
+ * norms, ordering, index build, join, pair kernel, mirror) into a graph on the
+ * first call and replay it on later calls with identical arguments (pointers,
+ * sizes, parameters and config; the stream may differ), keeping the 8 most
+ * recent graphs per context.  A replay reads the current contents of the caller's buffers.
+ * While graphs are on, profiling events are not recorded; launch counts are.
+ * Disabling synchronises the device and frees the graphs.
+ */
+int cms_graph_enable(cms_ctx* ctx, int enable);
+
+/*
  * Per-stage timing of the tiled path, for benchmarks.  When enabled, every
  * cms_cosine_greedy* call records a CUDA event pair on its stream around each
  * stage; cms_profile_read synchronises those events and returns, per stage,
