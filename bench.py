@@ -346,6 +346,18 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": join_ms,
                 "stage_ms_per_step": {n: float(v) / args.steps for n, v in zip(names, stage_ms)},
                 "dominant_stage": names[dom]}
+    # the cosine roofline of the build plan: peak visits a two-pointer sweep of
+    # every pair would make, sum over pairs of (n_ref + n_query) = Q * P_ref +
+    # R * P_query, per second of the join, against one visit per lane per clock
+    # (148 SMs x 128 lanes x max SM clock).  The indexed join skips most of that
+    # work, so this is an equivalence, not a count of what the kernel executes.
+    visits = (Q * ref.n_peaks + R * qry.n_peaks) * args.steps / join_launches
+    lane_peak = 148 * 128 * 1965e6
+    roofline["lane_issue_equivalent"] = {
+        "achieved_visits_per_s": visits / (join_ms / 1000.0), "peak_visits_per_s": lane_peak,
+        "frac": visits / (join_ms / 1000.0) / lane_peak,
+        "ncu_issue_active_pct": 50.0, "ncu_shared_pipe_pct": 23.0,
+        "ncu_source": "profiles/join_kernel_batched_cosine_20k.txt (20k x 20k capture)"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
