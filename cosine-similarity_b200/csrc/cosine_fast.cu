@@ -532,6 +532,30 @@ join_kernel(JoinParams P) {
         while (range_lo < q_end) {
             const int range_hi = min(range_lo + width, q_end);
             const int rw = range_hi - range_lo;
+            // ---- zeros for the dense row segment of the range: queries without
+            // a candidate keep them; the runs' results, stored by this warp
+            // after a __syncwarp, overwrite theirs (a spilled pair's overflow
+            // flag is rewritten by the pair kernel).  Four queries per lane,
+            // 16-byte streaming stores when aligned.
+            if (!SPARSE) {
+                const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
+                int qv = 0;
+                if ((row & 3) == 0 && (P.dense.ld & 3) == 0) {
+                    for (; qv + 128 <= rw; qv += 128) {
+                        const int64_t o = row + qv + 4 * lane;
+                        __stcs(reinterpret_cast<float4*>(P.dense.score + o),
+                               make_float4(0.f, 0.f, 0.f, 0.f));
+                        __stcs(reinterpret_cast<int4*>(P.dense.matches + o), make_int4(0, 0, 0, 0));
+                        __stcs(reinterpret_cast<uchar4*>(P.dense.overflow + o),
+                               make_uchar4(0, 0, 0, 0));
+                    }
+                }
+                for (int qr = qv + lane; qr < rw; qr += 32) {
+                    __stcs(&P.dense.score[row + qr], 0.f);
+                    __stcs(&P.dense.matches[row + qr], 0);
+                    __stcs(&P.dense.overflow[row + qr], (unsigned char)0);
+                }
+            }
             // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
             for (int w = 4 * lane; w < rw / 2 + 2; w += 128)
                 *reinterpret_cast<uint4*>(cnt + w) = make_uint4(0u, 0u, 0u, 0u);
@@ -907,60 +931,6 @@ join_kernel(JoinParams P) {
             }
             __syncwarp();
             flush_long();
-            // ---- zeros for the queries without a candidate ----
-            if (!SPARSE) {
-                // dense row segment out[a, b_begin + range_lo ...): the runs'
-                // results were stored as they were resolved; every other query
-                // of the range gets score 0, matches 0, and every query overflow
-                // 0 (a spilled pair's is rewritten by the pair kernel).  Four
-                // queries per lane, 16-byte streaming stores when aligned.
-                const int64_t row = (int64_t)a * P.dense.ld + b_begin + range_lo;
-                int qv = 0;
-                if ((row & 3) == 0 && (P.dense.ld & 3) == 0) {
-                    for (; qv + 128 <= rw; qv += 128) {
-                        const int q0 = qv + 4 * lane;
-                        // run ends of queries q0..q0+3 and of q0-1 (start of q0)
-                        unsigned e0 = 0, e1 = 0, e2 = 0, e3 = 0, sp = 0;
-                        if (n > 0) {
-                            const uint2 w = *reinterpret_cast<const uint2*>(cnt + (q0 >> 1));
-                            e0 = w.x & 0xFFFFu;
-                            e1 = w.x >> 16;
-                            e2 = w.y & 0xFFFFu;
-                            e3 = w.y >> 16;
-                            sp = q0 > 0 ? (cnt[(q0 >> 1) - 1] >> 16) : 0u;
-                        }
-                        __stcs(reinterpret_cast<uchar4*>(P.dense.overflow + row + q0),
-                               make_uchar4(0, 0, 0, 0));
-                        if (e3 == sp) {
-                            __stcs(reinterpret_cast<float4*>(P.dense.score + row + q0),
-                                   make_float4(0.f, 0.f, 0.f, 0.f));
-                            __stcs(reinterpret_cast<int4*>(P.dense.matches + row + q0),
-                                   make_int4(0, 0, 0, 0));
-                        } else {
-                            const unsigned st[4] = {sp, e0, e1, e2}, en[4] = {e0, e1, e2, e3};
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                if (en[k] == st[k]) {
-                                    __stcs(&P.dense.score[row + q0 + k], 0.f);
-                                    __stcs(&P.dense.matches[row + q0 + k], 0);
-                                }
-                            }
-                        }
-                    }
-                }
-                for (int qr = qv + lane; qr < rw; qr += 32) {
-                    bool empty = true;
-                    if (n > 0) {
-                        const unsigned e = cnt_get(cnt, qr);
-                        empty = e == (qr > 0 ? cnt_get(cnt, qr - 1) : 0u);
-                    }
-                    __stcs(&P.dense.overflow[row + qr], (unsigned char)0);
-                    if (empty) {
-                        __stcs(&P.dense.score[row + qr], 0.f);
-                        __stcs(&P.dense.matches[row + qr], 0);
-                    }
-                }
-            }
             __syncwarp();
             range_lo = range_hi;
             if (n < kPoolMax / 4) width = min(tn, width * 2);
