@@ -368,8 +368,8 @@ struct Pool {
 //                          scatter) ends of each query's run in perm
 //   n     int              candidates pushed in this sweep
 //   res   int2   [32]      per-lane staging of run results
-//   long  uint16 [kLongRuns] runs longer than 2 (resolved by the warp): runs of
-//                          3..kMidRun candidates from the front, longer ones
+//   long  uint16 [kLongRuns] runs longer than 3 (resolved by the warp): runs of
+//                          4..kMidRun candidates from the front, longer ones
 //                          from the back
 constexpr int kLongRuns = 64;
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
@@ -729,13 +729,13 @@ join_kernel(JoinParams P) {
             // where the query index changes.  The result of a run is packed
             // into the ckey slot of its first candidate: (score f32 bits,
             // matches), matches = -1 for a pair sent to the pair kernel.
-            // Queued runs of 3..32 candidates share the long_runs list: runs of
+            // Queued runs of 4..32 candidates share the long_runs list: runs of
             // at most kMidRun candidates from the front (start | (L-1) << 12),
             // longer ones from the back (start only).
             int n_mid = 0, n_big = 0;
             auto flush_long = [&]() {
                 __syncwarp();
-                // runs of 3..8 candidates, four at a time: each 8-lane segment
+                // runs of 4..8 candidates, four at a time: each 8-lane segment
                 // sorts one run's (key, gen) descending in registers (bitonic),
                 // then resolves it greedily by segment-wise ballot
                 const int seg = lane >> 3, t = lane & 7;
@@ -863,7 +863,7 @@ join_kernel(JoinParams P) {
                 n_mid = 0;
                 n_big = 0;
             };
-            // Runs of length 1 and 2 are resolved by their lane in closed
+            // Runs of 1 to 3 candidates are resolved by their lane in closed
             // form; longer runs (up to 32) are queued and resolved by the warp.
             for (int c = 0; c < n; c += 32) {
                 const int i = c + lane;
@@ -875,7 +875,7 @@ join_kernel(JoinParams P) {
                 }
                 int L = 0;
                 if (st) L = (int)cnt_get(cnt, q_i) - i;
-                const bool is_long = st && L > 2 && L <= kLongRun && L < P.match_limit;
+                const bool is_long = st && L > 3 && L <= kLongRun && L < P.match_limit;
                 const bool is_mid = is_long && L <= kMidRun;
                 const unsigned mb = __ballot_sync(full, is_mid);
                 const unsigned bb = __ballot_sync(full, is_long && !is_mid);
@@ -900,22 +900,43 @@ join_kernel(JoinParams P) {
                         const int s0 = pool.perm(i);
                         double score = pool.key(s0);
                         mt = 1;
-                        if (L == 2) {
+                        if (L >= 2) {
+                            // two or three candidates: sorting network, then greedy
                             const int s1 = pool.perm(i + 1);
-                            double k0 = score, k1 = pool.key(s1);
-                            uint32_t g0 = pool.gen(s0), g1 = pool.gen(s1);
-                            if (before(k1, g1, k0, g0)) {
-                                const double tk = k0;
-                                k0 = k1;
-                                k1 = tk;
-                                const uint32_t tg = g0;
-                                g0 = g1;
-                                g1 = tg;
+                            double k0 = score, k1 = pool.key(s1), k2 = 0.0;
+                            uint32_t g0 = pool.gen(s0), g1 = pool.gen(s1), g2 = 0;
+                            if (L == 3) {
+                                const int s2 = pool.perm(i + 2);
+                                k2 = pool.key(s2);
+                                g2 = pool.gen(s2);
+                            }
+                            auto order = [](double& ka, uint32_t& ga, double& kb, uint32_t& gb) {
+                                if (before(kb, gb, ka, ga)) {
+                                    const double tk = ka;
+                                    ka = kb;
+                                    kb = tk;
+                                    const uint32_t tg = ga;
+                                    ga = gb;
+                                    gb = tg;
+                                }
+                            };
+                            auto clash = [](uint32_t ga, uint32_t gb) {
+                                return (ga >> 16) == (gb >> 16) || (ga & 0xFFFFu) == (gb & 0xFFFFu);
+                            };
+                            order(k0, g0, k1, g1);
+                            if (L == 3) {
+                                order(k1, g1, k2, g2);
+                                order(k0, g0, k1, g1);
                             }
                             score = k0;
-                            if ((g0 >> 16) != (g1 >> 16) && (g0 & 0xFFFFu) != (g1 & 0xFFFFu)) {
+                            const bool take1 = !clash(g0, g1);
+                            if (take1) {
                                 score = __dadd_rn(score, k1);
                                 mt = 2;
+                            }
+                            if (L == 3 && !clash(g0, g2) && !(take1 && clash(g1, g2))) {
+                                score = __dadd_rn(score, k2);
+                                ++mt;
                             }
                         }
                         sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
