@@ -53,7 +53,7 @@ BYTES_PER_PAIR = 9
 # DRAM bytes per pair of join_kernel (read + write), from an ncu capture of the
 # 20k x 20k case of this workload (profiles/join_kernel_batched_cosine_20k.txt);
 # traffic grows with pairs, so a full launch is scaled by its pair count.
-JOIN_TRAFFIC_BYTES_PER_PAIR = 9.88
+JOIN_TRAFFIC_BYTES_PER_PAIR = 10.54
 
 
 def parse():
