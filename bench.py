@@ -356,7 +356,7 @@ def run_ours(args, world, rank, local):
     roofline["lane_issue_equivalent"] = {
         "achieved_visits_per_s": visits / (join_ms / 1000.0), "peak_visits_per_s": lane_peak,
         "frac": visits / (join_ms / 1000.0) / lane_peak,
-        "ncu_issue_active_pct": 50.0, "ncu_shared_pipe_pct": 23.0,
+        "ncu_issue_active_pct": 47.2, "ncu_shared_pipe_pct": 21.0,
         "ncu_source": "profiles/join_kernel_batched_cosine_20k.txt (20k x 20k capture)"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
