@@ -54,6 +54,10 @@ class PackedSpectra:
     intensity_power: float
     n_max_peaks: Optional[int]
     _device: dict = field(default_factory=dict, repr=False, compare=False)
+    # float32 intensities when b is exactly their float64 widening (intensity
+    # power 1, set by pack_csr): uploads then send 4 bytes a peak instead of 8
+    # and widen on the device
+    _b32: Optional[np.ndarray] = field(default=None, repr=False, compare=False)
 
     @property
     def n(self) -> int:
@@ -68,7 +72,9 @@ class PackedSpectra:
         return np.diff(self.offsets)
 
     def host_bytes(self) -> int:
-        return int(self.mz.nbytes + self.b.nbytes + self.offsets.nbytes
+        """Bytes that to_device copies from the host."""
+        b = self._b32 if self._b32 is not None and self._b32.shape == self.b.shape else self.b
+        return int(self.mz.nbytes + b.nbytes + self.offsets.nbytes
                    + (self.a.nbytes if self.a is not None else 0))
 
     def to_device(self, device, non_blocking: bool = False):
@@ -88,7 +94,11 @@ class PackedSpectra:
                     return None
                 return staging.upload(np.ascontiguousarray(x), device)
 
-            self._device[key] = DeviceSpectra(up(self.mz), up(self.a), up(self.b),
+            if self._b32 is not None and self._b32.shape == self.b.shape:
+                b = up(self._b32).to(torch.float64)
+            else:
+                b = up(self.b)
+            self._device[key] = DeviceSpectra(up(self.mz), up(self.a), b,
                                               up(self.offsets), self.n, self.n_peaks)
             if not non_blocking:
                 torch.cuda.current_stream(device).synchronize()
@@ -107,14 +117,16 @@ class PackedSpectra:
         seg = np.repeat(np.arange(self.n), keep)
         idx = self.offsets[:-1][seg] + (np.arange(off[-1]) - off[:-1][seg])
         return PackedSpectra(self.mz[idx], None if self.a is None else self.a[idx], self.b[idx],
-                             off, self.mz_power, self.intensity_power, int(n_max_peaks))
+                             off, self.mz_power, self.intensity_power, int(n_max_peaks),
+                             _b32=None if self._b32 is None else self._b32[idx])
 
     def subset(self, start: int, stop: int) -> "PackedSpectra":
         """Spectra [start, stop) as a new packed set (peaks re-based to 0)."""
         lo, hi = int(self.offsets[start]), int(self.offsets[stop])
         return PackedSpectra(self.mz[lo:hi], None if self.a is None else self.a[lo:hi],
                              self.b[lo:hi], self.offsets[start:stop + 1] - lo, self.mz_power,
-                             self.intensity_power, self.n_max_peaks)
+                             self.intensity_power, self.n_max_peaks,
+                             _b32=None if self._b32 is None else self._b32[lo:hi])
 
 
 @dataclass
@@ -185,7 +197,8 @@ def pack_csr(mz, intensities, offsets, n_max_peaks: Optional[int] = 1024,
                     raise ValueError("m/z values must be sorted ascending within each spectrum")
     a, b = _weights(mz32, int32, mz_power, intensity_power)
     return PackedSpectra(mz32, a, b, new_off, float(mz_power), float(intensity_power),
-                         None if n_max_peaks is None else int(n_max_peaks))
+                         None if n_max_peaks is None else int(n_max_peaks),
+                         _b32=int32 if float(intensity_power) == 1.0 else None)
 
 
 def pack_spectra(spectra: Sequence, n_max_peaks: Optional[int] = 1024, mz_power: float = 0.0,
