@@ -142,3 +142,31 @@ def test_autotune_sampling_matches_oracle_counts():
     assert cfg["mode"] == 1 and 32 <= cfg["tile_spectra"] <= 4096
     dense = autotune.WorkloadStats(500.0, 900.0, 1500.0, 1500.0)
     assert autotune.heuristic_config(dense, 1000)["mode"] == 2
+
+
+def test_mean_candidates_estimate_matches_exact_mean():
+    """The tuner's peak-level estimate of candidates per pair agrees with the
+    exact mean over every pair (window counts by the same rule as the kernels)
+    within a few percent, for the heavy-tailed benchmark distribution where a
+    sample of whole pairs is noisy."""
+    import numpy as np
+
+    from cudams import autotune, synthetic
+
+    r = synthetic.lognormal_spectra(400, seed=11)
+    q = synthetic.lognormal_spectra(300, seed=12)
+    exact = 0
+    mq = q.mz.astype(np.float64)
+    for i in range(r.n):
+        mr = r.mz[r.offsets[i]:r.offsets[i + 1]].astype(np.float64)
+        # candidates of reference spectrum i with every query spectrum at once
+        for j in range(q.n):
+            m = mq[q.offsets[j]:q.offsets[j + 1]]
+            exact += int((np.searchsorted(m, mr + 0.01, side="right")
+                          - np.searchsorted(m, mr - 0.01, side="left")).sum())
+    exact /= r.n * q.n
+    est = autotune.mean_candidates(r, q, 0.01)
+    assert abs(est - exact) / exact < 0.05, (est, exact)
+    # the heuristic turns it into ~128 candidates per work item
+    cfg = autotune.heuristic_config(autotune.WorkloadStats(est, 0.0, 99.0, 99.0), 100_000, 100_000)
+    assert abs(cfg["tile_spectra"] * est - autotune.CANDIDATES_PER_ITEM) < 32 * est + 1
