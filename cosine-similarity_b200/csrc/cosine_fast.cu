@@ -22,18 +22,24 @@
 //                        entries inside the tolerance window (the
 //                        two-pointer sweep of the reference, with the second
 //                        pointer advanced by the index instead of one step at
-//                        a time), test them exactly in float64 and push
-//                        candidates into a per-warp shared-memory pool.  The
-//                        pool is sorted by query, each query's short
-//                        candidate run is resolved greedily by one lane, and
-//                        the row segment is written coalesced.  Pairs with
-//                        long runs (or >= match_limit candidates) are
-//                        appended to a spill list.
+//                        a time), test them with exact float32 window bounds
+//                        and push candidates into a per-warp pool (shared
+//                        memory, extended in global memory).  The pool is
+//                        counting-sorted by query; each query's run is then
+//                        resolved greedily: 1-3 candidates in closed form by
+//                        one lane, 4-8 by an 8-lane segment, 9-32 by the warp.
+//                        The dense row segment is zeroed with coalesced
+//                        stores just before, and each run stores its result
+//                        over its zeros.  Pairs with longer runs (or >=
+//                        match_limit candidates) go to a spill list.
 //   6. pair_kernel       one CTA per spilled pair (or per pair of the whole
 //                        matrix in mode 2): exact generation-order sweep with
 //                        match_limit truncation, bitonic sort of (key, gen)
-//                        in shared memory, warp-parallel greedy with
-//                        used-peak bitmasks.
+//                        (in registers when there are eight candidates a
+//                        thread, else in shared memory), warp greedy with
+//                        per-chunk conflict masks and used-peak bitmasks.
+//   7. mirror_kernel     (symmetric dense calls, csrc/mirror.cu) lower
+//                        triangle copied from the upper one.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
