@@ -130,7 +130,30 @@ KNOWN = [
 ]
 
 
-def cosine_cases():
+def _mgf_spectra(path: Path):
+    """(m/z, intensity) float64 arrays of an MGF file's spectra: peaks sorted
+    by m/z, intensities scaled to a maximum of 1 (matchms'
+    normalize_intensities, which the reference's tests apply to their MGF
+    spectra before scoring)."""
+    spectra, cur, inside = [], [], False
+    for line in path.read_text(errors="replace").splitlines():
+        line = line.strip()
+        if line.upper() == "BEGIN IONS":
+            inside, cur = True, []
+        elif line.upper() == "END IONS":
+            inside = False
+            arr = np.array(cur, float).reshape(-1, 2)
+            arr = arr[np.argsort(arr[:, 0], kind="stable")]
+            if arr.shape[0] and arr[:, 1].max() > 0:
+                arr[:, 1] = arr[:, 1] / arr[:, 1].max()
+            spectra.append((arr[:, 0].copy(), arr[:, 1].copy()))
+        elif inside and line and (line[0].isdigit() or line[0] in "+-."):
+            parts = line.split()
+            cur.append((float(parts[0]), float(parts[1])))
+    return spectra
+
+
+def cosine_cases(reference: Path = None):
     rng = np.random.default_rng(20261203)
     cases = []
     for i, (s1, s2, tol, p, q) in enumerate(KNOWN):
@@ -167,6 +190,14 @@ def cosine_cases():
     cases.append(("limit_exact", [KNOWN[0][0]], [KNOWN[0][0]],
                   dict(tolerance=0.1, mz_power=0.0, intensity_power=1.0, shift=0.0,
                        match_limit=5, n_max_peaks=16)))
+    # measured spectra: the reference's own test data (tests/data/pesticides.mgf),
+    # all 76 against all 76 with the reference's default parameters
+    mgf = None if reference is None else reference / "tests" / "data" / "pesticides.mgf"
+    if mgf is not None and mgf.is_file():
+        pest = _mgf_spectra(mgf)
+        cases.append(("pesticides", pest, pest,
+                      dict(tolerance=0.1, mz_power=0.0, intensity_power=1.0, shift=0.0,
+                           match_limit=2048, n_max_peaks=1024)))
     return cases
 
 
@@ -198,11 +229,13 @@ def run_reference_cosine(Spectrum, CudaCosineGreedy, refs, qrys, params):
     return out[:, :len(refs), :len(qrys)]
 
 
-def make_cosine(reference: Path, Spectrum):
+def make_cosine(reference: Path, Spectrum, only_case=None):
     sys.path.insert(0, str(reference))
     from cudams.similarity import CudaCosineGreedy  # the reference package
 
-    for name, refs, qrys, params in cosine_cases():
+    for name, refs, qrys, params in cosine_cases(reference):
+        if only_case and name != only_case:
+            continue
         t = time.time()
         out = run_reference_cosine(Spectrum, CudaCosineGreedy, refs, qrys, params)
         rmz, rit, roff = _csr(refs)
@@ -258,6 +291,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--only", choices=["cosine", "fingerprint"], default=None)
+    ap.add_argument("--case", default=None, help="only this cosine case (e.g. pesticides)")
     args = ap.parse_args()
     ref = Path(args.reference)
     if not (ref / "cudams").is_dir():
@@ -268,7 +302,7 @@ def main():
     if args.only in (None, "fingerprint"):
         make_fingerprints(ref)
     if args.only in (None, "cosine"):
-        make_cosine(ref, Spectrum)
+        make_cosine(ref, Spectrum, args.case)
 
 
 if __name__ == "__main__":
