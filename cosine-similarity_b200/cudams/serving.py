@@ -230,6 +230,7 @@ class Server:
         # Measured here, not per request: querying the driver on the request
         # path serialises the worker threads.
         self._budget = self._free_bytes() - self.reserve_bytes
+        self._start_budget = self._budget
 
     # -- client side ------------------------------------------------------------
     def submit(self, queries, threshold: Optional[float] = None) -> Future:
@@ -276,8 +277,14 @@ class Server:
                     self.max_concurrent = max(self.max_concurrent, self._running)
                     return
                 if not remeasured:
-                    self._budget = (self._free_bytes() + self._in_flight_bytes
-                                    - self.reserve_bytes)
+                    # free memory plus what the running requests hold, but never
+                    # above the budget measured at start: an admitted request
+                    # may not have allocated yet, so free memory can overstate
+                    # what is left, and taken at face value it admits more
+                    # than fits
+                    self._budget = min(self._start_budget,
+                                       self._free_bytes() + self._in_flight_bytes
+                                       - self.reserve_bytes)
                     remeasured = True
                     continue
                 self._mem_lock.wait(timeout=0.05)
