@@ -346,7 +346,7 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": join_ms,
                 "stage_ms_per_step": {n: float(v) / args.steps for n, v in zip(names, stage_ms)},
                 "dominant_stage": names[dom]}
-    # the cosine roofline of the build plan: peak visits a two-pointer sweep of
+    # the lane-issue roofline of greedy cosine: peak visits a two-pointer sweep of
     # every pair would make, sum over pairs of (n_ref + n_query) = Q * P_ref +
     # R * P_query, per second of the join, against one visit per lane per clock
     # (148 SMs x 128 lanes x max SM clock).  The indexed join skips most of that
