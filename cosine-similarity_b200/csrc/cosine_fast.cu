@@ -1236,12 +1236,20 @@ __global__ void pair_kernel(PairParams P) {
             // Accepted keys are summed in sorted order, as the sequential greedy.
             if (wid == 0) {
                 const unsigned below = (1u << lane) - 1u;
+                // the next chunk's candidates are loaded while this one is
+                // resolved (they do not depend on the used-peak bits)
+                uint32_t g_nx = lane < n ? cgen[lane] : 0u;
+                unsigned long long k_nx = lane < n ? okey[lane] : 0ull;
                 for (int c = 0; c < n; c += 32) {
                     const int i = c + lane;
-                    uint32_t g = 0;
+                    const uint32_t g = g_nx;
+                    const unsigned long long ok = k_nx;
+                    if (i + 32 < n) {
+                        g_nx = cgen[i + 32];
+                        k_nx = okey[i + 32];
+                    }
                     bool alive = false;
                     if (i < n) {
-                        g = cgen[i];
                         const int p1 = g >> 16, p2 = g & 0xFFFF;
                         alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
                                 !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
@@ -1269,7 +1277,7 @@ __global__ void pair_kernel(PairParams P) {
                         atomicOr(&used_r[p1 >> 5], 1u << (p1 & 31));
                         atomicOr(&used_q[p2 >> 5], 1u << (p2 & 31));
                     }
-                    const double kk = (i < n) ? key_from_order(okey[i]) : 0.0;
+                    const double kk = (i < n) ? key_from_order(ok) : 0.0;
                     for (unsigned a = acc; a; a &= a - 1u) {
                         const double k = __shfl_sync(full, kk, __ffs(a) - 1);
                         score = __dadd_rn(score, k);
