@@ -54,6 +54,10 @@ BYTES_PER_PAIR = 9
 # 20k x 20k case of this workload (profiles/join_kernel_batched_cosine_20k.txt);
 # traffic grows with pairs, so a full launch is scaled by its pair count.
 JOIN_TRAFFIC_BYTES_PER_PAIR = 10.54
+# issue and shared-pipe utilisation of the same capture (quoted, not measured
+# by a bench run)
+JOIN_PROFILE = "profiles/join_kernel_batched_cosine_20k.txt (20k x 20k capture)"
+JOIN_PROFILE_FIGURES = {"issue_active_pct": 47.2, "shared_pipe_pct": 21.0}
 
 
 def parse():
@@ -134,6 +138,7 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
+        self._t = None
         self.lines = []
         self.t0 = self.t1 = None
 
@@ -166,6 +171,11 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+                self.proc.wait(timeout=5)
+            if self._t is not None:
+                self._t.join(timeout=5)
+            self.proc.stdout.close()
+            self.proc = None
 
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
@@ -201,6 +211,27 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except (OSError, ValueError, KeyError):
         return 6650.0, "fallback"
+
+
+def sm_max_mhz(clock_summary=None):
+    """Maximum SM clock: MEASURED_PEAKS.json's record when it has one, else the
+    clocks.max.sm that nvidia-smi reported during the run."""
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        for k, v in d.items():
+            if "sm" in k.lower() and "max" in k.lower() and "mhz" in k.lower():
+                return float(v), "MEASURED_PEAKS.json " + k
+    except (OSError, ValueError, TypeError):
+        pass
+    if clock_summary and clock_summary.get("sm_max_mhz"):
+        return float(clock_summary["sm_max_mhz"]), "nvidia-smi clocks.max.sm"
+    return 1965.0, "B200 nominal clocks.max.sm"
+
+
+def sm_count(dev):
+    import torch
+
+    return int(torch.cuda.get_device_properties(dev).multi_processor_count)
 
 
 # ----------------------------------------------------------------------------
@@ -352,12 +383,16 @@ def run_ours(args, world, rank, local):
     # (148 SMs x 128 lanes x max SM clock).  The indexed join skips most of that
     # work, so this is an equivalence, not a count of what the kernel executes.
     visits = (Q * ref.n_peaks + R * qry.n_peaks) * args.steps / join_launches
-    lane_peak = 148 * 128 * 1965e6
+    clk = clocks.summary()
+    mhz, mhz_src = sm_max_mhz(clk)
+    n_sm = sm_count(dev)
+    lane_peak = n_sm * 128 * mhz * 1e6
     roofline["lane_issue_equivalent"] = {
         "achieved_visits_per_s": visits / (join_ms / 1000.0), "peak_visits_per_s": lane_peak,
         "frac": visits / (join_ms / 1000.0) / lane_peak,
-        "ncu_issue_active_pct": 47.2, "ncu_shared_pipe_pct": 21.0,
-        "ncu_source": "profiles/join_kernel_batched_cosine_20k.txt (20k x 20k capture)"}
+        "peak_basis": f"{n_sm} SMs (device properties) x 128 lanes x {mhz:.0f} MHz ({mhz_src})",
+        "ncu_profile": {"note": "not measured by this run: figures of the committed ncu capture",
+                        "source": JOIN_PROFILE, **JOIN_PROFILE_FIGURES}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -367,7 +402,7 @@ def run_ours(args, world, rank, local):
                        "tuning": cfg, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"row shards x{world}, no collective"},
             "gpu_launches": int(stage_n.sum()),
-            "roofline": roofline, "clocks": clocks.summary()}
+            "roofline": roofline, "clocks": clk}
 
     # plain comparator (same inputs, row sample)
     if not args.no_plain:
@@ -478,7 +513,8 @@ def other_workloads(dev, args):
     tms = _time_ms(torch_jaccard)
     del R, Q
     torch.cuda.empty_cache()
-    popc_peak = 148 * 16 * 1965e6 / 2  # 64-bit popcounts/s at 16 POPC32 per clock per SM
+    mhz, _ = sm_max_mhz()
+    popc_peak = sm_count(dev) * 16 * mhz * 1e6 / 2  # popc64/s at 16 POPC32 per clock per SM
     res["fingerprint_100k"] = {
         "workload": f"{n_fp} x {n_fp} fingerprints, 2048 bits, density U(5%,15%)",
         "pairs_per_s": fp, "unit": "pairs/s",

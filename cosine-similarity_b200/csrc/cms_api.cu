@@ -1,6 +1,8 @@
 // Context, errors and scratch management of libcudams_b200.so.
 #include <cstdarg>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "cms_internal.cuh"
@@ -71,6 +73,39 @@ bool check_specset(const SpecSet& s, const char* name) {
         return false;
     }
     return true;
+}
+
+int raise_func_smem(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set_to;
+    int dev = 0;
+    CMS_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = set_to[{dev, func}];
+    if (bytes <= cur) return CMS_OK;
+    CMS_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes));
+    cur = bytes;
+    return CMS_OK;
+}
+
+int check_device_ptr(const void* p, const char* who, const char* what) {
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        set_error("%s: %s is not a CUDA pointer (%s)", who, what, cudaGetErrorString(e));
+        return CMS_ERR_INVALID;
+    }
+    if (at.type == cudaMemoryTypeManaged) return CMS_OK;
+    int dev = 0;
+    CMS_CUDA_TRY(cudaGetDevice(&dev));
+    if (at.type != cudaMemoryTypeDevice || at.device != dev) {
+        set_error("%s: %s must be device memory of the current device %d (memory type %d, "
+                  "device %d)", who, what, dev, (int)at.type, at.device);
+        return CMS_ERR_INVALID;
+    }
+    return CMS_OK;
 }
 
 static cudaEvent_t pool_event(cms_ctx* ctx) {

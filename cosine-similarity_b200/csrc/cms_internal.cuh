@@ -130,6 +130,17 @@ inline size_t bump_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
 bool check_specset(const SpecSet& s, const char* name);
 
+// Raise a kernel's cudaFuncAttributeMaxDynamicSharedMemorySize on the current
+// device to at least `bytes`, never lowering it.  The attribute is process
+// wide, so a call that lowered it could make a concurrent call's launch (on
+// another host thread, with a larger need) fail between its set and its
+// launch; a monotone value under one mutex cannot.
+int raise_func_smem(const void* func, size_t bytes);
+
+// CMS_OK when `p` is device (or managed) memory that the current device can
+// use in a kernel, else CMS_ERR_INVALID with a message naming `what`.
+int check_device_ptr(const void* p, const char* who, const char* what);
+
 // Scope that counts `n` launches for a profiling stage and, when profiling
 // is on, records an event pair around them on stream `s`.
 class StageScope {

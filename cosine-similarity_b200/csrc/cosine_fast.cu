@@ -1381,15 +1381,15 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
 }
 
 template <typename T>
-void set_func_smem(T* f, size_t bytes) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+int set_func_smem(T* f, size_t bytes) {
+    return raise_func_smem(reinterpret_cast<const void*>(f), bytes);
 }
 
 template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
 int launch_join(cms_ctx* ctx, const JoinParams& jp, size_t smem, size_t gpool_warps,
                 cudaStream_t s, int max_grid = 0) {
     auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT>;
-    set_func_smem(kern, smem);
+    if (const int rc = set_func_smem(kern, smem)) return rc;
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
     int grid = ctx->sm_count * std::max(1, per_sm);
@@ -1518,11 +1518,11 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
 
     int pair_blocks_per_sm = 1;
     if (sparse) {
-        set_func_smem(pair_kernel<true>, pair_smem);
+        if ((rc = set_func_smem(pair_kernel<true>, pair_smem))) return rc;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<true>,
                                                       p.pair_threads, pair_smem);
     } else {
-        set_func_smem(pair_kernel<false>, pair_smem);
+        if ((rc = set_func_smem(pair_kernel<false>, pair_smem))) return rc;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<false>,
                                                       p.pair_threads, pair_smem);
     }
@@ -1891,8 +1891,31 @@ extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_
         set_error("cms_cosine_greedy_noalloc: null output pointer");
         return CMS_ERR_INVALID;
     }
+    // Every buffer must be memory of the current device: the scratch address
+    // below is the current device's, and a kernel handed another GPU's (or
+    // host) memory would read or write out of bounds.  Nothing is launched
+    // before these checks.
+    const char* who = "cms_cosine_greedy_noalloc";
+    const std::pair<const void*, const char*> bufs[] = {
+        {ref_mz, "ref_mz"}, {ref_a, "ref_a"}, {ref_b, "ref_b"}, {ref_off, "ref_off"},
+        {q_mz, "q_mz"},     {q_a, "q_a"},     {q_b, "q_b"},     {q_off, "q_off"},
+        {score, "score"},   {matches, "matches"}, {overflow, "overflow"},
+        {device_error, "device_error"}};
+    int rc = CMS_OK;
+    for (const auto& bf : bufs)
+        if (bf.first && (rc = check_device_ptr(bf.first, who, bf.second))) return rc;
+    if (s) {
+        int sdev = -1, dev = 0;
+        CMS_CUDA_TRY(cudaStreamGetDevice(s, &sdev));
+        CMS_CUDA_TRY(cudaGetDevice(&dev));
+        if (sdev != dev) {
+            set_error("%s: stream belongs to device %d, not the current device %d", who, sdev,
+                      dev);
+            return CMS_ERR_INVALID;
+        }
+    }
     unsigned char* base = nullptr;
-    int rc = noalloc_scratch(&base);
+    rc = noalloc_scratch(&base);
     if (rc) return rc;
     uint32_t* bad = reinterpret_cast<uint32_t*>(base);
     uint32_t* err = reinterpret_cast<uint32_t*>(base + 4);
@@ -1936,9 +1959,7 @@ extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_
     pp.bad = bad;
     const int pair_threads = 128;
     const size_t pair_smem = (size_t)cap * 12 + 2 * 2048 * 4;
-    CMS_CUDA_TRY(cudaFuncSetAttribute(pair_kernel<false>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)pair_smem));
+    if ((rc = set_func_smem(pair_kernel<false>, pair_smem))) return rc;
     int per_sm = 1;
     CMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<false>,
                                                                pair_threads, pair_smem));
@@ -2209,9 +2230,7 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     pp.bad = bad;
     {
         StageScope sc(ctx, 4, 1, s);
-        CMS_CUDA_TRY(cudaFuncSetAttribute(pair_kernel<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)pair_smem));
+        if ((rc = set_func_smem(pair_kernel<true>, pair_smem))) return rc;
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<true>, 128, pair_smem);
         pair_kernel<true><<<std::max(1, std::min(ctx->sm_count * std::max(1, per_sm),

@@ -151,10 +151,12 @@ fingerprint_kernel(FpParams P) {
 }
 
 template <int MEASURE>
-void launch_fp(dim3 grid, size_t smem, cudaStream_t s, const FpParams& P) {
-    cudaFuncSetAttribute(fingerprint_kernel<MEASURE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+int launch_fp(dim3 grid, size_t smem, cudaStream_t s, const FpParams& P) {
+    if (const int rc = raise_func_smem(reinterpret_cast<const void*>(fingerprint_kernel<MEASURE>),
+                                       smem))
+        return rc;
     fingerprint_kernel<MEASURE><<<grid, kFpThreads, smem, s>>>(P);
+    return CMS_OK;
 }
 
 }  // namespace
@@ -189,17 +191,19 @@ int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
     dim3 grid((unsigned)gx, (unsigned)gy);
     cudaStream_t s = (cudaStream_t)stream;
     const size_t smem = (size_t)(kBM + kBN) * kLd * sizeof(uint64_t);
+    int rc = CMS_OK;
     switch (measure) {
         case CMS_FP_JACCARD:
-            launch_fp<CMS_FP_JACCARD>(grid, smem, s, P);
+            rc = launch_fp<CMS_FP_JACCARD>(grid, smem, s, P);
             break;
         case CMS_FP_DICE:
-            launch_fp<CMS_FP_DICE>(grid, smem, s, P);
+            rc = launch_fp<CMS_FP_DICE>(grid, smem, s, P);
             break;
         default:
-            launch_fp<CMS_FP_COSINE>(grid, smem, s, P);
+            rc = launch_fp<CMS_FP_COSINE>(grid, smem, s, P);
             break;
     }
+    if (rc) return rc;
     CMS_CUDA_TRY(cudaGetLastError());
     if (sym) {
         int dev = 0, sms = 148;

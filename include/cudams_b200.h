@@ -241,9 +241,15 @@ int cms_library_destroy(cms_library* lib);
  *     one float64 norm per spectrum); every GPU that loads the library holds
  *     it until the process exits.  Limit: n_ref + n_q <= 1048576 spectra and
  *     match_limit <= 4096; larger calls fail with CMS_ERR_UNSUPPORTED.
+ *   - Device: every pointer argument must be memory of the CURRENT device
+ *     (cudaSetDevice before the call; managed memory is accepted) and the
+ *     stream, when not NULL, must belong to it.  Otherwise the call returns
+ *     CMS_ERR_INVALID before launching anything.
  *   - The first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress) and caches it; make that first call before any
- *     stream capture begins.
+ *     stream capture begins.  The cache assumes that the device's primary
+ *     context lives for the whole process: after cudaDeviceReset the cached
+ *     address is stale, so do not call this entry point again after a reset.
  *   - All calls share the one array, and it keeps the last call's contents
  *     (the call clears the flags it needs): calls that overlap on the GPU,
  *     from different streams or host threads, race and corrupt each other.

@@ -1,9 +1,10 @@
 """Generate golden fixtures from the reference implementation itself.
 
-Run in a container where the reference is mounted (read-only) at
-/root/reference:
+Run where the reference package (a checkout of tornikeo/cosine-similarity)
+is readable; its root is given by --reference or, when that is omitted, by
+the CUDAMS_REFERENCE environment variable (one of the two is required):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path to the checkout>
 
 Greedy cosine: the reference's Numba kernel (cudams/similarity/
 spectrum_similarity_functions.py:39-278) is run under numba's CUDA simulator
@@ -289,10 +290,13 @@ def make_fingerprints(reference: Path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("CUDAMS_REFERENCE"),
+                    help="root of the reference checkout (default: $CUDAMS_REFERENCE)")
     ap.add_argument("--only", choices=["cosine", "fingerprint"], default=None)
     ap.add_argument("--case", default=None, help="only this cosine case (e.g. pesticides)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set CUDAMS_REFERENCE to the reference checkout")
     ref = Path(args.reference)
     if not (ref / "cudams").is_dir():
         sys.exit(f"reference package not found under {ref}")

@@ -7,9 +7,11 @@ may imply, or a plugin host that forbids allocations behind its back.  This
 entry point serves them from a fixed device array compiled into the library.
 The test calls it through the C ABI twice in a row on different inputs (so a
 second call must not see the first call's leftovers in the shared array) and
-checks each result bit for bit against cms_cosine_greedy, the way every other
-parity test here compares outputs.  It also checks that a call larger than
-the array is refused with a clear error instead of touching the GPU.
+checks each result bit for bit twice: against the CPU oracle (the check every
+parity test here makes) and against the regular entry point
+cms_cosine_greedy.  It also checks that a call larger than the array, and a
+call whose output is host memory, are refused with a clear error before any
+kernel runs.
 
 This file is named so that pytest collects it last.
 """
@@ -46,6 +48,12 @@ def _noalloc(rd, qd, tol, shift, match_limit):
     return tuple(t.cpu().numpy() for t in out), int(err.item())
 
 
+def _oracle(r, q, tol, shift, match_limit):
+    from oracle import oracle
+
+    return oracle.cosine_greedy(r, q, tol, shift, match_limit)
+
+
 def _regular(rd, qd, tol, shift, match_limit):
     from cudams import kernels
 
@@ -57,19 +65,21 @@ def test_noalloc_equals_regular_entry_two_calls(cuda_device):
     from cudams import synthetic
 
     # call 1: the 1024 x 1024-workload distribution at ragged sizes
-    r1 = synthetic.uniform_spectra(301, seed=41).to_device(cuda_device)
-    q1 = synthetic.uniform_spectra(257, seed=42).to_device(cuda_device)
+    h1 = synthetic.uniform_spectra(301, seed=41), synthetic.uniform_spectra(257, seed=42)
+    r1, q1 = (x.to_device(cuda_device) for x in h1)
     got1, err1 = _noalloc(r1, q1, 0.1, 0.0, 2048)
     assert err1 == 0
-    assert_same(got1, _regular(r1, q1, 0.1, 0.0, 2048), "noalloc call 1")
+    assert_same(got1, _oracle(*h1, 0.1, 0.0, 2048), "noalloc call 1 vs oracle")
+    assert_same(got1, _regular(r1, q1, 0.1, 0.0, 2048), "noalloc call 1 vs cms_cosine_greedy")
 
     # call 2, right after: other sizes, powers, shift and match_limit
-    r2 = synthetic.uniform_spectra(150, seed=43, mz_power=0.5, intensity_power=2.0)
-    q2 = synthetic.uniform_spectra(410, seed=44, mz_power=0.5, intensity_power=2.0)
-    r2, q2 = r2.to_device(cuda_device), q2.to_device(cuda_device)
+    h2 = (synthetic.uniform_spectra(150, seed=43, mz_power=0.5, intensity_power=2.0),
+          synthetic.uniform_spectra(410, seed=44, mz_power=0.5, intensity_power=2.0))
+    r2, q2 = (x.to_device(cuda_device) for x in h2)
     got2, err2 = _noalloc(r2, q2, 0.3, 0.25, 7)
     assert err2 == 0
-    assert_same(got2, _regular(r2, q2, 0.3, 0.25, 7), "noalloc call 2")
+    assert_same(got2, _oracle(*h2, 0.3, 0.25, 7), "noalloc call 2 vs oracle")
+    assert_same(got2, _regular(r2, q2, 0.3, 0.25, 7), "noalloc call 2 vs cms_cosine_greedy")
     assert got2[2].any()  # match_limit 7: some pairs overflow
 
 
@@ -90,3 +100,26 @@ def test_noalloc_rejects_oversized_call(cuda_device):
         ptr(out), ptr(out), ptr(out), 1, None, None)
     assert rc == _native.CMS_ERR_UNSUPPORTED
     assert "exceeds the fixed scratch capacity" in _native.last_error()
+
+
+def test_noalloc_rejects_host_output(cuda_device):
+    """An output buffer in host memory is refused before any launch: the
+    entry point only accepts memory of the current device."""
+    import torch
+
+    from cudams import _native, synthetic
+    from cudams._native import ptr
+
+    lib = _native.load()
+    d = synthetic.uniform_spectra(3, seed=46).to_device(cuda_device)
+    host_score = np.full((3, 3), -5.0, np.float32)
+    m = torch.zeros((3, 3), dtype=torch.int32, device=cuda_device)
+    o = torch.zeros((3, 3), dtype=torch.uint8, device=cuda_device)
+    rc = lib.cms_cosine_greedy_noalloc(
+        ptr(d.mz), ptr(d.a), ptr(d.b), ptr(d.offsets), d.n, d.n_peaks,
+        ptr(d.mz), ptr(d.a), ptr(d.b), ptr(d.offsets), d.n, d.n_peaks, 0.1, 0.0, 10,
+        ctypes.c_void_p(host_score.ctypes.data), ptr(m), ptr(o), 3, None, None)
+    assert rc == _native.CMS_ERR_INVALID
+    assert "score must be device memory of the current device" in _native.last_error()
+    torch.cuda.synchronize()
+    assert (host_score == -5.0).all()
