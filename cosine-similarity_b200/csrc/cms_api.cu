@@ -167,6 +167,19 @@ int cms_graph_enable(cms_ctx* ctx, int enable) {
     return CMS_OK;
 }
 
+int cms_trace_enable(cms_ctx* ctx, uint64_t* records, int64_t capacity, uint64_t* count,
+                     uint32_t tag) {
+    if (!ctx || (records && (!count || capacity < 0))) {
+        cms::set_error("cms_trace_enable: null context or invalid trace buffer");
+        return CMS_ERR_INVALID;
+    }
+    ctx->trace_rec = reinterpret_cast<unsigned long long*>(records);
+    ctx->trace_count = reinterpret_cast<unsigned long long*>(count);
+    ctx->trace_cap = records ? capacity : 0;
+    ctx->trace_tag = tag;
+    return CMS_OK;
+}
+
 int cms_profile_read(cms_ctx* ctx, double* stage_ms, int64_t* stage_launches, int reset) {
     if (!ctx) {
         cms::set_error("cms_profile_read: null context");

@@ -103,6 +103,11 @@ struct cms_ctx {
     // graphs are captured on this stream (capture is not allowed on the legacy
     // default stream) and launched on the caller's
     cudaStream_t capture_stream = nullptr;
+    // join-kernel work-item trace (cms_trace_enable); rec null: off
+    unsigned long long* trace_rec = nullptr;
+    unsigned long long* trace_count = nullptr;
+    long long trace_cap = 0;
+    unsigned int trace_tag = 0;
 };
 
 namespace cms {

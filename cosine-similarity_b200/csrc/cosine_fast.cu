@@ -28,6 +28,11 @@
 //                        counting-sorted by query; each query's run is then
 //                        resolved greedily: 1-3 candidates in closed form by
 //                        one lane, 4-8 by an 8-lane segment, 9-32 by the warp.
+//                        The sweep is load-balanced: a chunk's window entries
+//                        are expanded 32 at a time over the warp, and each
+//                        query's candidates are chained through a per-warp
+//                        head table (tagged by an epoch, so it is rarely
+//                        cleared) instead of being counting-sorted.
 //                        The dense row segment is zeroed with coalesced
 //                        stores just before, and each run stores its result
 //                        over its zeros.  Pairs with longer runs (or >=
@@ -281,6 +286,21 @@ __device__ __forceinline__ void emit_hit(const SparseOut& o, int r, int q, float
     }
 }
 
+// Optional per-work-item timing records (cms_trace_enable): 4 words each --
+// tag | smid << 32, item index, %globaltimer at its start and end (ns).
+struct TraceOut {
+    unsigned long long* rec;
+    unsigned long long* count;
+    long long cap;
+    unsigned int tag;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 struct SpillList {
     int2* pairs;  // (reference, query)
     unsigned int* count;
@@ -311,8 +331,14 @@ struct JoinParams {
     double shift;
     int match_limit;
     float init_width_scale;  // first sub-range width = scale / n_A_peaks (0: whole tile)
+    // first sub-range width per length class of the sweeping spectrum (the
+    // tuner's measured candidate-pool split); 0: init_width_scale decides
+    int width_by_class[kOrderClasses];
     int warp_smem_bytes;     // per-warp slice of dynamic shared memory
-    unsigned char* gpool;    // global pool extension, kGPool * 16 bytes per warp
+    int pool_max;            // candidates a sweep may hold: kPoolMax, or kPool without gpool
+    int max_fetch;           // fetches of kFetch items per warp before it exits (0: no limit)
+    unsigned char* gpool;    // global pool extension, kGPool * 16 bytes per warp (or null)
+    TraceOut trace;          // per-item timing records (rec null: off)
     unsigned long long* work;
     SpillList spill;
     DenseOut dense;
@@ -322,10 +348,20 @@ struct JoinParams {
     int sym;  // only pairs (reference i, query j) with i <= j
 };
 
-constexpr int kFetch = 4;  // work items taken per atomic
+constexpr int kFetch = 4;                  // work items taken per atomic
+constexpr int kSearchFetches = 4;          // fetches per warp of a library search's CTAs
 constexpr int kPoolMax = 4096;             // candidates per sweep: smem pool + global extension
 constexpr int kGPool = kPoolMax - kPool;   // global extension entries per warp
-static_assert(kPoolMax <= 4096, "queued run starts are packed into 12 bits");
+static_assert(kPoolMax <= 4096, "pool slots are packed into 12 bits");
+static_assert(kMaxTile <= 4096, "query indices within a range are packed into 12 bits");
+
+// Candidate metadata word: the query's index within the swept range (bits
+// 0-11) and the slot of the previous candidate of the same query (bits 12-23,
+// present when kHasNext is set).  A query's candidates form a chain that
+// starts at the slot its head names (the candidate pushed last).
+constexpr uint32_t kHasNext = 1u << 24;
+__device__ __forceinline__ int meta_query(uint32_t m) { return (int)(m & 0xFFFu); }
+__device__ __forceinline__ int meta_next(uint32_t m) { return (int)((m >> 12) & 0xFFFu); }
 
 // A warp's candidate pool: the first kPool entries live in shared memory, the
 // rest in a per-warp slice of global scratch (L2-resident), so that a large
@@ -334,64 +370,45 @@ static_assert(kPoolMax <= 4096, "queued run starts are packed into 12 bits");
 struct Pool {
     double* skey;
     uint32_t* sgen;
-    uint16_t* scq;
-    uint16_t* sperm;
+    uint32_t* smeta;
     double* gkey;
     uint32_t* ggen;
-    uint16_t* gcq;
-    uint16_t* gperm;
+    uint32_t* gmeta;
     __device__ __forceinline__ double key(int i) const { return i < kPool ? skey[i] : gkey[i - kPool]; }
     __device__ __forceinline__ uint32_t gen(int i) const { return i < kPool ? sgen[i] : ggen[i - kPool]; }
-    __device__ __forceinline__ int cq(int i) const { return i < kPool ? scq[i] : gcq[i - kPool]; }
-    __device__ __forceinline__ int perm(int i) const { return i < kPool ? sperm[i] : gperm[i - kPool]; }
-    __device__ __forceinline__ void put(int i, double k, uint32_t g, int q) const {
+    __device__ __forceinline__ uint32_t meta(int i) const {
+        return i < kPool ? smeta[i] : gmeta[i - kPool];
+    }
+    __device__ __forceinline__ void put(int i, double k, uint32_t g, uint32_t m) const {
         if (i < kPool) {
             skey[i] = k;
             sgen[i] = g;
-            scq[i] = (uint16_t)q;
+            smeta[i] = m;
         } else {
             gkey[i - kPool] = k;
             ggen[i - kPool] = g;
-            gcq[i - kPool] = (uint16_t)q;
+            gmeta[i - kPool] = m;
         }
-    }
-    __device__ __forceinline__ void set_perm(int pos, int slot) const {
-        if (pos < kPool)
-            sperm[pos] = (uint16_t)slot;
-        else
-            gperm[pos - kPool] = (uint16_t)slot;
     }
 };
 
-// Per-warp shared-memory slice (offsets in bytes; the count array's length
+// Per-warp shared-memory slice (offsets in bytes; the head table's length
 // depends on the tile size, so the slice size is computed at launch).
-//   ckey  double [kPool]   candidate key
-//   cgen  uint32 [kPool]   (p_ref << 16) | p_query
-//   cq    uint16 [kPool]   query index within the current sub-range
-//   perm  uint16 [kPool]   candidate slots grouped by query
-//   cnt   uint32 [tile/2+1] two 16-bit counters per word: per-query counts,
-//                          then (after the scan) starts, then (after the
-//                          scatter) ends of each query's run in perm
-//   n     int              candidates pushed in this sweep
-//   res   int2   [32]      per-lane staging of run results
-//   long  uint16 [kLongRuns] runs longer than 3 (resolved by the warp): runs of
-//                          4..kMidRun candidates from the front, longer ones
-//                          from the back
+//   key   double [kPool]     candidate key
+//   gen   uint32 [kPool]     (p_ref << 16) | p_query
+//   meta  uint32 [kPool]     query in range | previous candidate of the query
+//   head  uint32 [tile/2]    two 16-bit heads per word, one per query of the
+//                            range: (epoch << 12) | slot of its last candidate;
+//                            a head of another epoch means "no candidate yet"
+//   wa    double [32]        per-lane sweeping-peak weight of the current chunk
+//   lh    float2 [32]        per-lane float32 window [L, H] of the current chunk
+//   runs  uint32 [kLongRuns] runs of 4..32 candidates queued for the warp:
+//                            slot of the chain head | length << 12; runs of at
+//                            most kMidRun from the front, longer ones from the back
 constexpr int kLongRuns = 64;
+__host__ __device__ constexpr int head_words(int tile) { return (((tile + 1) / 2) + 3) & ~3; }
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
-    // counters: tile/2 + 1 words are used; the 16-byte zeroing may touch up
-    // to tile/2 + 5, so round that up to whole uint4s
-    return ((16 * kPool + 4 * (((tile / 2 + 5) + 3) & ~3) + 2 * kLongRuns + 8 * 32 + 16) + 15) &
-           ~15;
-}
-
-__device__ __forceinline__ unsigned cnt_get(const uint32_t* w, int q) {
-    return (w[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-}
-// counts never exceed kPool (< 2^16), so a half never carries into the other
-__device__ __forceinline__ unsigned cnt_inc(uint32_t* w, int q) {
-    const unsigned sh = (unsigned)(q & 1) * 16u;
-    return (atomicAdd(&w[q >> 1], 1u << sh) >> sh) & 0xFFFFu;
+    return 16 * kPool + 4 * head_words(tile) + 8 * 32 + 8 * 32 + 4 * kLongRuns;
 }
 
 // Exact float32 window of one sweeping peak.
@@ -456,46 +473,44 @@ struct Window {
     }
 };
 
-// Three CTAs (24 warps) per SM: up to 85 registers a thread.  Measured on the
-// 20k x 20k lognormal case: 5% faster than four CTAs at 64 registers (which
-// spill more) and 13% faster than two CTAs (too few warps to hide latency).
+// Three CTAs (24 warps) per SM: up to 85 registers a thread.
 template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
 __global__ void __launch_bounds__(kJoinThreads, 3)
 join_kernel(JoinParams P) {
     if (*P.bad) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int hw = head_words(P.g.tile);
     unsigned char* slice = smem_raw + (size_t)(threadIdx.x >> 5) * P.warp_smem_bytes;
-    double* ckey = reinterpret_cast<double*>(slice);
-    uint32_t* cgen = reinterpret_cast<uint32_t*>(slice + 8 * kPool);
-    uint16_t* cq = reinterpret_cast<uint16_t*>(slice + 12 * kPool);
-    uint16_t* perm = reinterpret_cast<uint16_t*>(slice + 14 * kPool);
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(slice + 16 * kPool);
-    int* n_ptr = reinterpret_cast<int*>(slice + P.warp_smem_bytes - 16);
-    uint16_t* long_runs = reinterpret_cast<uint16_t*>(slice + P.warp_smem_bytes - 16 - 8 * 32 -
-                                                      2 * kLongRuns);
+    uint32_t* head = reinterpret_cast<uint32_t*>(slice + 16 * kPool);
+    double* s_wa = reinterpret_cast<double*>(slice + 16 * kPool + 4 * hw);
+    float2* s_lh = reinterpret_cast<float2*>(slice + 16 * kPool + 4 * hw + 8 * 32);
+    uint32_t* long_runs = reinterpret_cast<uint32_t*>(slice + 16 * kPool + 4 * hw + 16 * 32);
     Pool pool;
     {
         const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
-        unsigned char* g = P.gpool + gw * (size_t)kGPool * 16;
-        pool.skey = ckey;
-        pool.sgen = cgen;
-        pool.scq = cq;
-        pool.sperm = perm;
+        unsigned char* g = P.gpool ? P.gpool + gw * (size_t)kGPool * 16 : nullptr;
+        pool.skey = reinterpret_cast<double*>(slice);
+        pool.sgen = reinterpret_cast<uint32_t*>(slice + 8 * kPool);
+        pool.smeta = reinterpret_cast<uint32_t*>(slice + 12 * kPool);
         pool.gkey = reinterpret_cast<double*>(g);
-        pool.ggen = reinterpret_cast<uint32_t*>(g + 8 * kGPool);
-        pool.gcq = reinterpret_cast<uint16_t*>(g + 12 * kGPool);
-        pool.gperm = reinterpret_cast<uint16_t*>(g + 14 * kGPool);
+        pool.ggen = reinterpret_cast<uint32_t*>(g ? g + 8 * kGPool : nullptr);
+        pool.gmeta = reinterpret_cast<uint32_t*>(g ? g + 12 * kGPool : nullptr);
     }
 
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
+    const unsigned below = (1u << lane) - 1u;
     const int64_t nA = P.A.n;
     const int64_t n_items = nA * (int64_t)P.g.n_tiles;
     const unsigned nbmask = (unsigned)(P.g.nb - 1);
     const Entry* __restrict__ ent = P.ent;
     const uint32_t* __restrict__ tab = P.tab;
+    // epoch of the head table (1..15): every swept range takes the next one,
+    // so heads left by earlier ranges read as empty without clearing the
+    // table; it is cleared once per 15 ranges (and before the first)
+    unsigned epoch = 15;
 
-    for (;;) {
+    for (int fetches = 0; P.max_fetch == 0 || fetches < P.max_fetch; ++fetches) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(P.work, (unsigned long long)kFetch);
         base = __shfl_sync(full, base, 0);
@@ -507,6 +522,7 @@ join_kernel(JoinParams P) {
             ai -= nA;
             ++tt;
         }
+        const unsigned long long t_item = P.trace.rec ? global_ns() : 0ull;
         const int t = (int)tt;
         const int a = P.a_order[ai];
         const int64_t a0 = P.A.off[a];
@@ -522,9 +538,23 @@ join_kernel(JoinParams P) {
             __stcs(&P.dense.score[o], sc);
             __stcs(&P.dense.matches[o], mt);
         };
+        auto store_result = [&](int bq, double score, int mt) {
+            const double snB = P.snB[bq];
+            const float sc =
+                (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA));
+            if (SPARSE) {
+                if (sc >= P.sparse.threshold)
+                    emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
+            } else {
+                put_dense(bq, sc, mt);
+            }
+        };
 
         int width = tn;
-        if (P.init_width_scale > 0.f && na > 0)  // multiples of 32 keep row writes aligned
+        const int wc = P.width_by_class[length_class(na)];
+        if (wc > 0)
+            width = max(1, min(tn, wc));
+        else if (P.init_width_scale > 0.f && na > 0)  // multiples of 32 keep row writes aligned
             width = max(32, min(tn, (int)(P.init_width_scale / (float)na) & ~31));
         // queries of this item: the whole tile, or under `sym` those on or
         // above the diagonal (reference index <= query index)
@@ -538,12 +568,20 @@ join_kernel(JoinParams P) {
         while (range_lo < q_end) {
             const int range_hi = min(range_lo + width, q_end);
             const int rw = range_hi - range_lo;
-            // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
-            for (int w = 4 * lane; w < rw / 2 + 2; w += 128)
-                *reinterpret_cast<uint4*>(cnt + w) = make_uint4(0u, 0u, 0u, 0u);
-            if (lane == 0) *n_ptr = 0;
+            epoch = epoch == 15 ? 1u : epoch + 1u;
+            if (epoch == 1u)
+                for (int w = 4 * lane; w < hw; w += 128)
+                    *reinterpret_cast<uint4*>(head + w) = make_uint4(0u, 0u, 0u, 0u);
             __syncwarp();
-            // the next chunk's peaks are loaded while this chunk is swept
+            // ---- sweep: candidates of (a, queries [range_lo, range_hi)) ----
+            // Each lane takes one sweeping peak of a 32-peak chunk and finds
+            // the tile-stream entries of its window's buckets (one run, or two
+            // when the hashed bucket range wraps).  The chunk's entries are
+            // then processed 32 at a time, flat entry k by lane k % 32, which
+            // finds the peak that owns it by a binary search over the warp's
+            // inclusive entry counts: every lane tests an entry in every
+            // round, however unevenly the entries fall among the peaks.
+            int n = 0;  // candidates found (warp-uniform)
             float nx_mz = 0.f;
             double nx_w = 0.0;
             if (lane < na) {
@@ -558,94 +596,121 @@ join_kernel(JoinParams P) {
                     nx_mz = P.A.mz[a0 + p + 32];
                     nx_w = __dmul_rn(peak_a(P.A.a, a0 + p + 32), P.A.b[a0 + p + 32]);
                 }
+                float L = 1.0f, H = 0.0f;
+                uint32_t r0b = 0, c0 = 0, r1b = 0, c1 = 0;
                 if (p < na) {
-                    float L, H;
                     if (!Window<A_IS_REF, NOSHIFT>::bounds(mzA, P.tol, P.shift, L, H)) {
                         atomicOr(P.err, kErrBadOffsets);
                         L = 1.0f;
                         H = 0.0f;
                     }
-                    // the window's buckets are one contiguous run of the tile
-                    // stream, or two when the hashed range wraps around
-                    uint32_t r0b = 0, r0e = 0, r1b = 0, r1e = 0;
                     if (L <= H) {
                         const long long blo = bucket_of(L, P.g.inv_w);
                         const long long bhi = bucket_of(H, P.g.inv_w);
                         if (bhi - blo + 1 >= P.g.nb) {
                             r0b = __ldg(&T[0]);
-                            r0e = __ldg(&T[P.g.nb]);
+                            c0 = __ldg(&T[P.g.nb]) - r0b;
                         } else {
                             const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
                             r0b = __ldg(&T[bl]);
                             if (bl <= bh) {
-                                r0e = __ldg(&T[bh + 1]);
+                                c0 = __ldg(&T[bh + 1]) - r0b;
                             } else {
-                                r0e = __ldg(&T[P.g.nb]);
+                                c0 = __ldg(&T[P.g.nb]) - r0b;
                                 r1b = __ldg(&T[0]);
-                                r1e = __ldg(&T[bh + 1]);
-                            }
-                        }
-                    }
-                    uint32_t e = r0b, ee = r0e;
-                    for (;;) {
-                        if (e >= ee) {
-                            if (r1e == 0) break;
-                            e = r1b;
-                            ee = r1e;
-                            r1e = 0;
-                            continue;
-                        }
-                        // up to four entries per round trip
-                        Entry en[4];
-                        const int cntE = (int)min(4u, ee - e);
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-                            if (u < cntE) en[u] = ent[tbase + e + u];
-                        e += cntE;
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            if (u >= cntE) break;
-                            const int bq = (int)(en[u].id >> 16);
-                            if (!(en[u].mz >= L) || !(en[u].mz <= H) || bq < range_lo ||
-                                bq >= range_hi)
-                                continue;
-                            const int pB = (int)(en[u].id & 0xFFFFu);
-                            const double aB = P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
-                            double key;
-                            uint32_t gen;
-                            if (A_IS_REF) {
-                                key = __dmul_rn(__dmul_rn(wA, aB), en[u].b);
-                                gen = ((uint32_t)p << 16) | (uint32_t)pB;
-                            } else {
-                                const double wB = __dmul_rn(aB, en[u].b);
-                                key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + p)),
-                                                P.A.b[a0 + p]);
-                                gen = ((uint32_t)pB << 16) | (uint32_t)p;
-                            }
-                            // one pool reservation per group of lanes that found a
-                            // candidate together
-                            const int slot = atomicAdd(n_ptr, 1);
-                            if (slot < kPoolMax) {
-                                const int qr = bq - range_lo;
-                                pool.put(slot, key, gen, qr);
-                                cnt_inc(cnt, qr);
+                                c1 = __ldg(&T[bh + 1]) - r1b;
                             }
                         }
                     }
                 }
+                s_wa[lane] = wA;
+                s_lh[lane] = make_float2(L, H);
+                const uint32_t c = c0 + c1;
+                uint32_t incl = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t v = __shfl_up_sync(full, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                const uint32_t excl = incl - c;
+                const uint32_t E = __shfl_sync(full, incl, 31);
+                const bool wrapped = __any_sync(full, c1 != 0u);
+                const uint32_t off0 = r0b - excl;  // entry k of lane l: r0b + (k - excl)
                 __syncwarp();
-                const int n_now = *(volatile int*)n_ptr;
-                __syncwarp();
-                if (n_now > kPoolMax) break;
+                for (uint32_t kb = 0; kb < E; kb += 32) {
+                    const uint32_t k = kb + (uint32_t)lane;
+                    int o = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const uint32_t v = __shfl_sync(full, incl, o + step - 1);
+                        if (v <= k) o += step;
+                    }
+                    uint32_t pos;
+                    if (!wrapped) {
+                        pos = __shfl_sync(full, off0, o & 31) + k;
+                    } else {
+                        const uint32_t oex = __shfl_sync(full, excl, o & 31);
+                        const uint32_t oc0 = __shfl_sync(full, c0, o & 31);
+                        const uint32_t or0 = __shfl_sync(full, r0b, o & 31);
+                        const uint32_t or1 = __shfl_sync(full, r1b, o & 31);
+                        const uint32_t e = k - oex;
+                        pos = e < oc0 ? or0 + e : or1 + (e - oc0);
+                    }
+                    bool cand = false;
+                    Entry en;
+                    en.id = 0;
+                    if (k < E) {
+                        en = ent[tbase + pos];
+                        const float2 lh = s_lh[o];
+                        const int bq = (int)(en.id >> 16);
+                        cand = en.mz >= lh.x && en.mz <= lh.y && bq >= range_lo && bq < range_hi;
+                    }
+                    const unsigned bal = __ballot_sync(full, cand);
+                    const int slot = n + __popc(bal & below);
+                    n += __popc(bal);
+                    if (cand && slot < P.pool_max) {
+                        const int bq = (int)(en.id >> 16);
+                        const int pB = (int)(en.id & 0xFFFFu);
+                        const int pa = pc + o;
+                        const double aB = P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
+                        double key;
+                        uint32_t gen;
+                        if (A_IS_REF) {
+                            key = __dmul_rn(__dmul_rn(s_wa[o], aB), en.b);
+                            gen = ((uint32_t)pa << 16) | (uint32_t)pB;
+                        } else {
+                            const double wB = __dmul_rn(aB, en.b);
+                            key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + pa)), P.A.b[a0 + pa]);
+                            gen = ((uint32_t)pB << 16) | (uint32_t)pa;
+                        }
+                        // push onto the query's chain: swap the new slot into
+                        // its 16-bit head; the old head, if of this epoch, is
+                        // the chain's next element
+                        const int qr = bq - range_lo;
+                        uint32_t* hp = head + (qr >> 1);
+                        const unsigned sh = (unsigned)(qr & 1) * 16u;
+                        const unsigned nh = (epoch << 12) | (unsigned)slot;
+                        unsigned cur = *reinterpret_cast<volatile uint32_t*>(hp), assumed, ph;
+                        do {
+                            assumed = cur;
+                            ph = (assumed >> sh) & 0xFFFFu;
+                            cur = atomicCAS(hp, assumed, (assumed & ~(0xFFFFu << sh)) | (nh << sh));
+                        } while (cur != assumed);
+                        uint32_t m = (uint32_t)qr;
+                        if ((ph >> 12) == epoch) m |= ((ph & 0xFFFu) << 12) | kHasNext;
+                        pool.put(slot, key, gen, m);
+                    }
+                    if (n > P.pool_max) break;
+                }
+                __syncwarp();  // s_wa / s_lh are rewritten by the next chunk
+                if (n > P.pool_max) break;
             }
             __syncwarp();
-            const int n = *(volatile int*)n_ptr;
-            if (n > kPoolMax) {
+            if (n > P.pool_max) {
                 if (rw > 1) {
                     // too many candidates for one pool: retry a narrower range
-                    width = max(1, (int)((long long)rw * kPoolMax / (2LL * n)));
+                    width = max(1, (int)((long long)rw * P.pool_max / (2LL * n)));
                     width = min(width, rw / 2 > 0 ? rw / 2 : 1);
-                    __syncwarp();
                     continue;
                 }
                 // a single pair has more candidates than the pool: pair kernel
@@ -666,54 +731,6 @@ join_kernel(JoinParams P) {
                 continue;
             }
 
-            if (n > 0) {
-                // ---- counting sort of the pool by query ----
-                // exclusive scan of the per-query counts, in place (words of
-                // two): each step, lane l takes the uint4 (eight counters) at
-                // word 4 * l of a 128-word stripe, so a step's 32 accesses are
-                // consecutive 16-byte words (no bank conflicts); the stripe's
-                // total carries into the next step
-                const int nw = (rw / 2 + 1 + 3) & ~3;  // whole uint4s (zeroed beyond)
-                unsigned carry = 0;
-                for (int w = 4 * lane; w - 4 * lane < nw; w += 128) {
-                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                    if (w < nw) v = *reinterpret_cast<const uint4*>(cnt + w);
-                    const unsigned c0 = v.x & 0xFFFFu, c1 = v.x >> 16, c2 = v.y & 0xFFFFu,
-                                   c3 = v.y >> 16, c4 = v.z & 0xFFFFu, c5 = v.z >> 16,
-                                   c6 = v.w & 0xFFFFu, c7 = v.w >> 16;
-                    const unsigned local = c0 + c1 + c2 + c3 + c4 + c5 + c6 + c7;
-                    unsigned incl = local;
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const unsigned u = __shfl_up_sync(full, incl, d);
-                        if (lane >= d) incl += u;
-                    }
-                    unsigned run = carry + incl - local;
-                    uint4 o;
-                    o.x = run | ((run + c0) << 16);
-                    run += c0 + c1;
-                    o.y = run | ((run + c2) << 16);
-                    run += c2 + c3;
-                    o.z = run | ((run + c4) << 16);
-                    run += c4 + c5;
-                    o.w = run | ((run + c6) << 16);
-                    if (w < nw) *reinterpret_cast<uint4*>(cnt + w) = o;
-                    carry += __shfl_sync(full, incl, 31);
-                }
-                __syncwarp();
-                // scatter: the counters become run ends
-                for (int sl = lane; sl < n; sl += 32) pool.set_perm(cnt_inc(cnt, pool.cq(sl)), sl);
-                __syncwarp();
-            }
-
-            // ---- resolve each query's run, compactly: one lane per run ----
-            // Runs are contiguous in perm and ordered by query; a run starts
-            // where the query index changes.  The result of a run is packed
-            // into the ckey slot of its first candidate: (score f32 bits,
-            // matches), matches = -1 for a pair sent to the pair kernel.
-            // Queued runs of 4..32 candidates share the long_runs list: runs of
-            // at most kMidRun candidates from the front (start | (L-1) << 12),
-            // longer ones from the back (start only).
             // ---- zeros for the dense row segment of the range: queries without
             // a candidate keep them; the runs' results, stored by this warp
             // after the __syncwarp below, overwrite theirs (a spilled pair's
@@ -742,23 +759,30 @@ join_kernel(JoinParams P) {
                 }
             }
             __syncwarp();
+
+            // ---- resolve each query's run ----
+            // Slot s owns its query's run when the query's head names it (it
+            // was pushed last); the owner walks the chain.  Runs of 1 to 3
+            // candidates are resolved by their lane in closed form; runs of
+            // 4..32 are queued and resolved by the warp; longer runs (or runs
+            // reaching match_limit) go to the pair kernel.
             int n_mid = 0, n_big = 0;
             auto flush_long = [&]() {
                 __syncwarp();
                 // runs of 4..8 candidates, four at a time: each 8-lane segment
                 // sorts one run's (key, gen) descending in registers (bitonic),
                 // then resolves it greedily by segment-wise ballot
-                const int seg = lane >> 3, t = lane & 7;
+                const int seg = lane >> 3, tq = lane & 7;
                 for (int r = 0; r < n_mid; r += 4) {
                     const bool valid = r + seg < n_mid;
-                    const unsigned e = valid ? (unsigned)long_runs[r + seg] : 0u;
-                    const int i0 = (int)(e & 0xFFFu);
-                    const int L = valid ? (int)(e >> 12) + 1 : 0;
+                    const unsigned e = valid ? long_runs[r + seg] : 0u;
+                    const int s0 = (int)(e & 0xFFFu);
+                    const int L = valid ? (int)(e >> 12) : 0;
                     double k = -INFINITY;
                     uint32_t g = 0;
-                    int sl = 0;
-                    if (t < L) {
-                        sl = pool.perm(i0 + t);
+                    if (tq < L) {
+                        int sl = s0;
+                        for (int h = 0; h < tq; ++h) sl = meta_next(pool.meta(sl));
                         k = pool.key(sl);
                         g = pool.gen(sl);
                     }
@@ -768,8 +792,8 @@ join_kernel(JoinParams P) {
                         for (int j = kk >> 1; j > 0; j >>= 1) {
                             const double ok = __shfl_xor_sync(full, k, j);
                             const uint32_t og = __shfl_xor_sync(full, g, j);
-                            const bool lower = (t & j) == 0;
-                            const bool desc = (t & kk) == 0;
+                            const bool lower = (tq & j) == 0;
+                            const bool desc = (tq & kk) == 0;
                             const bool mine_first = before(k, g, ok, og);
                             const bool keep = (lower == desc) ? mine_first : !mine_first;
                             if (!keep) {
@@ -778,7 +802,7 @@ join_kernel(JoinParams P) {
                             }
                         }
                     }
-                    bool alive = t < L;
+                    bool alive = tq < L;
                     unsigned bal = __ballot_sync(full, alive);
                     double score = 0.0;
                     int mt = 0;
@@ -796,31 +820,19 @@ join_kernel(JoinParams P) {
                         }
                         bal = __ballot_sync(full, alive);
                     }
-                    if (valid && t == 0) {
-                        // sl is still the slot of the run's first candidate:
-                        // the sort moved keys and gens only
-                        const int q0 = pool.cq(sl);
-                        const int bq = b_begin + range_lo + q0;
-                        const double snB = P.snB[bq];
-                        const float sc = (float)__ddiv_rn(
-                            score, A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA));
-                        if (SPARSE) {
-                            if (sc >= P.sparse.threshold)
-                                emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
-                        } else {
-                            put_dense(bq, sc, mt);
-                        }
-                    }
+                    if (valid && tq == 0)
+                        store_result(b_begin + range_lo + meta_query(pool.meta(s0)), score, mt);
                 }
                 // runs of 9..32 candidates, one at a time on the whole warp
                 for (int r = 0; r < n_big; ++r) {
-                    const int i0 = long_runs[kLongRuns - 1 - r];
-                    const int q0 = pool.cq(pool.perm(i0));
-                    const int L = (int)cnt_get(cnt, q0) - i0;
+                    const unsigned e = long_runs[kLongRuns - 1 - r];
+                    const int s0 = (int)(e & 0xFFFu);
+                    const int L = (int)(e >> 12);
                     double k = -INFINITY;
                     uint32_t g = 0;
                     if (lane < L) {
-                        const int sl = pool.perm(i0 + lane);
+                        int sl = s0;
+                        for (int h = 0; h < lane; ++h) sl = meta_next(pool.meta(sl));
                         k = pool.key(sl);
                         g = pool.gen(sl);
                     }
@@ -856,70 +868,71 @@ join_kernel(JoinParams P) {
                             alive = false;
                         bal = __ballot_sync(full, alive);
                     }
-                    if (lane == 0) {
-                        const int bq = b_begin + range_lo + q0;
-                        const double snB = P.snB[bq];
-                        const float sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
-                                                                          : __dmul_rn(snB, snA));
-                        if (SPARSE) {
-                            if (sc >= P.sparse.threshold)
-                                emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
-                        } else {
-                            put_dense(bq, sc, mt);
-                        }
-                    }
+                    if (lane == 0)
+                        store_result(b_begin + range_lo + meta_query(pool.meta(s0)), score, mt);
                 }
                 __syncwarp();
                 n_mid = 0;
                 n_big = 0;
             };
-            // Runs of 1 to 3 candidates are resolved by their lane in closed
-            // form; longer runs (up to 32) are queued and resolved by the warp.
             for (int c = 0; c < n; c += 32) {
-                const int i = c + lane;
-                bool st = false;
-                int q_i = 0;
-                if (i < n) {
-                    q_i = pool.cq(pool.perm(i));
-                    st = (i == 0) || (pool.cq(pool.perm(i - 1)) != q_i);
+                const int s = c + lane;
+                bool own = false;
+                int L = 0, qr = 0;
+                double k0 = 0.0, k1 = 0.0, k2 = 0.0;
+                uint32_t g0 = 0, g1 = 0, g2 = 0;
+                if (s < n) {
+                    const uint32_t m0 = pool.meta(s);
+                    qr = meta_query(m0);
+                    const unsigned h = (head[qr >> 1] >> ((qr & 1) * 16)) & 0xFFFu;
+                    own = h == (unsigned)s;
+                    if (own) {
+                        k0 = pool.key(s);
+                        g0 = pool.gen(s);
+                        L = 1;
+                        if (m0 & kHasNext) {
+                            const int s1 = meta_next(m0);
+                            const uint32_t m1 = pool.meta(s1);
+                            k1 = pool.key(s1);
+                            g1 = pool.gen(s1);
+                            L = 2;
+                            if (m1 & kHasNext) {
+                                const int s2 = meta_next(m1);
+                                uint32_t m2 = pool.meta(s2);
+                                k2 = pool.key(s2);
+                                g2 = pool.gen(s2);
+                                L = 3;
+                                // longer runs: count the rest (up to kLongRun + 1)
+                                while ((m2 & kHasNext) && L <= kLongRun) {
+                                    m2 = pool.meta(meta_next(m2));
+                                    ++L;
+                                }
+                            }
+                        }
+                    }
                 }
-                int L = 0;
-                if (st) L = (int)cnt_get(cnt, q_i) - i;
-                const bool is_long = st && L > 3 && L <= kLongRun && L < P.match_limit;
+                const bool is_long = own && L > 3 && L <= kLongRun && L < P.match_limit;
                 const bool is_mid = is_long && L <= kMidRun;
                 const unsigned mb = __ballot_sync(full, is_mid);
                 const unsigned bb = __ballot_sync(full, is_long && !is_mid);
                 if (n_mid + n_big + __popc(mb) + __popc(bb) > kLongRuns) flush_long();
-                const unsigned below = (1u << lane) - 1u;
+                const unsigned run = (unsigned)s | ((unsigned)L << 12);
                 if (is_mid)
-                    long_runs[n_mid + __popc(mb & below)] = (uint16_t)(i | ((L - 1) << 12));
+                    long_runs[n_mid + __popc(mb & below)] = run;
                 else if (is_long)
-                    long_runs[kLongRuns - 1 - (n_big + __popc(bb & below))] = (uint16_t)i;
+                    long_runs[kLongRuns - 1 - (n_big + __popc(bb & below))] = run;
                 n_mid += __popc(mb);
                 n_big += __popc(bb);
-                if (st && !is_long) {
-                    const int bq = b_begin + range_lo + q_i;
-                    float sc;
-                    int mt;
+                if (own && !is_long) {
+                    const int bq = b_begin + range_lo + qr;
                     if (L >= P.match_limit || L > kLongRun) {
                         spill_push(P.spill, A_IS_REF ? a : bq, A_IS_REF ? bq : a, P.err);
-                        sc = __int_as_float(0x7fc00000);
-                        mt = -1;
+                        if (!SPARSE) put_dense(bq, __int_as_float(0x7fc00000), -1);
                     } else {
-                        const double snB = P.snB[bq];
-                        const int s0 = pool.perm(i);
-                        double score = pool.key(s0);
-                        mt = 1;
+                        // one to three candidates: sorting network, then greedy
+                        double score = k0;
+                        int mt = 1;
                         if (L >= 2) {
-                            // two or three candidates: sorting network, then greedy
-                            const int s1 = pool.perm(i + 1);
-                            double k0 = score, k1 = pool.key(s1), k2 = 0.0;
-                            uint32_t g0 = pool.gen(s0), g1 = pool.gen(s1), g2 = 0;
-                            if (L == 3) {
-                                const int s2 = pool.perm(i + 2);
-                                k2 = pool.key(s2);
-                                g2 = pool.gen(s2);
-                            }
                             auto order = [](double& ka, uint32_t& ga, double& kb, uint32_t& gb) {
                                 if (before(kb, gb, ka, ga)) {
                                     const double tk = ka;
@@ -949,14 +962,7 @@ join_kernel(JoinParams P) {
                                 ++mt;
                             }
                         }
-                        sc = (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB)
-                                                              : __dmul_rn(snB, snA));
-                    }
-                    if (SPARSE) {
-                        if (mt > 0 && sc >= P.sparse.threshold)
-                            emit_hit(P.sparse, A_IS_REF ? a : bq, A_IS_REF ? bq : a, sc, mt, 0);
-                    } else {
-                        put_dense(bq, sc, mt);
+                        store_result(bq, score, mt);
                     }
                 }
             }
@@ -964,9 +970,21 @@ join_kernel(JoinParams P) {
             flush_long();
             __syncwarp();
             range_lo = range_hi;
-            if (n < kPoolMax / 4) width = min(tn, width * 2);
+            if (n < P.pool_max / 4) width = min(tn, width * 2);
         }
         __syncwarp();
+        if (P.trace.rec && lane == 0) {
+            const unsigned long long k = atomicAdd(P.trace.count, 1ull);
+            if ((long long)k < P.trace.cap) {
+                unsigned int smid;
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+                unsigned long long* r = P.trace.rec + 4 * k;
+                r[0] = (unsigned long long)P.trace.tag | ((unsigned long long)smid << 32);
+                r[1] = base + (unsigned long long)f;
+                r[2] = t_item;
+                r[3] = global_ns();
+            }
+        }
         }
     }
 }
@@ -1325,6 +1343,7 @@ struct Plan {
     unsigned int spill_cap;
     int sym;               // cms_cosine_config.symmetric
     double cand_per_pair;  // cms_cosine_config.cand_per_pair (0: unknown)
+    int width_by_class[kOrderClasses];  // cms_cosine_config.width_by_class
 };
 
 int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse, Plan& p) {
@@ -1376,6 +1395,14 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
     long long sc = std::max<long long>(1 << 20, pairs / 64);
     sc = std::min<long long>(sc, std::min<long long>(pairs, 1LL << 28));
     p.spill_cap = (unsigned int)std::max<long long>(sc, 1);
+    for (int c = 0; c < kOrderClasses; ++c) {
+        const int w = cfg ? cfg->width_by_class[c] : 0;
+        if (w < 0) {
+            set_error("cms_cosine_greedy: width_by_class entries must be >= 0");
+            return CMS_ERR_INVALID;
+        }
+        p.width_by_class[c] = w;
+    }
     (void)sparse;
     return CMS_OK;
 }
@@ -1385,20 +1412,36 @@ int set_func_smem(T* f, size_t bytes) {
     return raise_func_smem(reinterpret_cast<const void*>(f), bytes);
 }
 
+// Launch the join.  Persistent (jp.max_fetch == 0): one resident CTA per
+// slot, each warp pulling work until none is left; its warps own the global
+// pool slices, so the grid may not exceed the resident CTAs.  Bounded
+// (jp.max_fetch > 0, no global pool): enough short-lived CTAs for the work,
+// each warp exiting after max_fetch fetches, so that the SMs free up CTA by
+// CTA and concurrent launches on other streams are scheduled in between.
 template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
-int launch_join(cms_ctx* ctx, const JoinParams& jp, size_t smem, size_t gpool_warps,
-                cudaStream_t s, int max_grid = 0) {
+int launch_join(cms_ctx* ctx, JoinParams jp, size_t smem, size_t gpool_warps, int64_t n_items,
+                cudaStream_t s) {
     auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT>;
     if (const int rc = set_func_smem(kern, smem)) return rc;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
-    int grid = ctx->sm_count * std::max(1, per_sm);
-    if (max_grid > 0) grid = std::min(grid, max_grid);
-    if ((size_t)grid * kJoinWarps > gpool_warps) {
-        set_error("cms_cosine_greedy: join grid larger than its scratch");
-        return CMS_ERR_CUDA;
+    jp.trace = TraceOut{ctx->trace_rec, ctx->trace_count, ctx->trace_cap, ctx->trace_tag};
+    int64_t grid;
+    if (jp.max_fetch > 0) {
+        const int64_t per_cta = (int64_t)kJoinWarps * kFetch * jp.max_fetch;
+        grid = std::max<int64_t>(1, (n_items + per_cta - 1) / per_cta);
+        if (grid > INT32_MAX) {
+            set_error("cms_cosine_greedy: too many work items for one launch");
+            return CMS_ERR_UNSUPPORTED;
+        }
+    } else {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
+        grid = (int64_t)ctx->sm_count * std::max(1, per_sm);
+        if ((size_t)grid * kJoinWarps > gpool_warps) {
+            set_error("cms_cosine_greedy: join grid larger than its scratch");
+            return CMS_ERR_CUDA;
+        }
     }
-    kern<<<grid, kJoinThreads, smem, s>>>(jp);
+    kern<<<(unsigned)grid, kJoinThreads, smem, s>>>(jp);
     CMS_CUDA_TRY(cudaGetLastError());
     return CMS_OK;
 }
@@ -1577,6 +1620,7 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.shift = args.shift;
     jp.match_limit = args.match_limit;
     jp.init_width_scale = 0.f;
+    for (int c = 0; c < kOrderClasses; ++c) jp.width_by_class[c] = p.width_by_class[c];
     if (p.cand_per_pair > 0.0 && args.ref.n > 0) {
         // expected candidates of (A spectrum with n peaks, w queries) ~ n*w*lambda
         const double mean_na = (double)args.ref.n_peaks / (double)args.ref.n;
@@ -1584,6 +1628,8 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
     }
     jp.warp_smem_bytes = warp_slice_bytes(p.tile);
+    jp.pool_max = kPoolMax;
+    jp.max_fetch = 0;
     jp.gpool = gpool;
     jp.work = work_join;
     jp.spill = SpillList{spill, spill_count, p.spill_cap};
@@ -1596,10 +1642,13 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     {
         StageScope sc(ctx, 3, 1, s);
         const bool noshift = args.shift == 0.0;
-        rc = sparse ? (noshift ? launch_join<true, true, true>(ctx, jp, join_smem, gpool_warps, s)
-                               : launch_join<true, true, false>(ctx, jp, join_smem, gpool_warps, s))
-                    : (noshift ? launch_join<true, false, true>(ctx, jp, join_smem, gpool_warps, s)
-                               : launch_join<true, false, false>(ctx, jp, join_smem, gpool_warps, s));
+        const int64_t items = nR * (int64_t)p.n_tiles;
+        rc = sparse
+                 ? (noshift ? launch_join<true, true, true>(ctx, jp, join_smem, gpool_warps, items, s)
+                            : launch_join<true, true, false>(ctx, jp, join_smem, gpool_warps, items, s))
+                 : (noshift ? launch_join<true, false, true>(ctx, jp, join_smem, gpool_warps, items, s)
+                            : launch_join<true, false, false>(ctx, jp, join_smem, gpool_warps, items,
+                                                              s));
         if (rc) return rc;
     }
     CMS_CUDA_TRY(cudaGetLastError());
@@ -1678,8 +1727,13 @@ int run_cosine_graph(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense
     put(p.spill_cap);
     put(p.sym);
     put(p.cand_per_pair);
+    for (int c = 0; c < kOrderClasses; ++c) put(p.width_by_class[c]);
     put((uintptr_t)ctx->scratch.ptr);
     put(ctx->scratch.bytes);
+    put((uintptr_t)ctx->trace_rec);
+    put((uintptr_t)ctx->trace_count);
+    put(ctx->trace_cap);
+    put(ctx->trace_tag);
 
     auto& cache = ctx->graph_cache;
     for (size_t i = 0; i < cache.size(); ++i) {
@@ -2135,11 +2189,9 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     const long long items = (long long)n_q * lib->g.n_tiles;
     const unsigned int spill_cap =
         (unsigned int)std::min<long long>(std::max<long long>(1 << 16, items), 1 << 24);
-    const size_t gpool_warps = (size_t)ctx->sm_count * 64;
-    const size_t gpool_bytes = gpool_warps * (size_t)kGPool * 16;
     size_t need = bump_size(64 * sizeof(uint64_t)) + bump_size(n_q * sizeof(double)) +
                   bump_size(n_q * sizeof(int32_t)) + bump_size((size_t)spill_cap * sizeof(int2)) +
-                  bump_size(gpool_bytes) + 4096;
+                  4096;
     int rc = arena_reserve(ctx, ctx->scratch, need, s);
     if (rc) return rc;
     Bump bp{(char*)ctx->scratch.ptr, 0, ctx->scratch.bytes};
@@ -2153,7 +2205,6 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     double* snQ = bp.take<double>(n_q);
     int32_t* order = bp.take<int32_t>(n_q);
     int2* spill = bp.take<int2>(spill_cap);
-    unsigned char* gpool = bp.take<unsigned char>(gpool_bytes);
     CMS_CUDA_TRY(cudaMemsetAsync(small, 0, 64 * sizeof(uint64_t), s));
 
     const int threads = 256;
@@ -2176,7 +2227,7 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
 
     SparseOut so{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
                  reinterpret_cast<unsigned long long*>(hit_count), threshold};
-    JoinParams jp{};
+    JoinParams jp{};  // width_by_class zero: widths from cand_per_pair
     jp.A = Q;
     jp.B = lib->spec;
     jp.snA = snQ;
@@ -2188,14 +2239,19 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     jp.tol = lib->tol;
     jp.shift = lib->shift;
     jp.match_limit = lib->match_limit;
+    // A search runs as short-lived CTAs (bounded fetches per warp) so that
+    // searches on other streams interleave with it on the device; without
+    // resident warps there is no global pool, only the shared-memory one.
+    jp.pool_max = kPool;
+    jp.max_fetch = kSearchFetches;
     jp.init_width_scale = 0.f;
     if (lib->cand_per_pair > 0.0 && n_q > 0) {
         const double mean_na = (double)n_q_peaks / (double)n_q;
         const double lambda = lib->cand_per_pair / std::max(1.0, mean_na);
-        jp.init_width_scale = (float)(0.5 * kPoolMax / lambda);
+        jp.init_width_scale = (float)(0.5 * jp.pool_max / lambda);
     }
     jp.warp_smem_bytes = warp_slice_bytes(lib->g.tile);
-    jp.gpool = gpool;
+    jp.gpool = nullptr;
     jp.work = work_join;
     jp.spill = SpillList{spill, spill_count, spill_cap};
     jp.dense = DenseOut{nullptr, nullptr, nullptr, 0};
@@ -2203,12 +2259,9 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     jp.err = ctx->err_word;
     jp.bad = bad;
     {
-        // a small batch takes only the CTAs it can keep busy, leaving the
-        // rest of the GPU to batches running concurrently on other streams
-        const int max_grid = (int)std::max<long long>(ctx->sm_count, (items + 63) / 64);
         StageScope sc(ctx, 3, 1, s);
-        rc = launch_join<false, true, false>(ctx, jp, (size_t)jp.warp_smem_bytes * kJoinWarps,
-                                             gpool_warps, s, max_grid);
+        rc = launch_join<false, true, false>(ctx, jp, (size_t)jp.warp_smem_bytes * kJoinWarps, 0,
+                                             items, s);
         if (rc) return rc;
     }
     PairParams pp{};

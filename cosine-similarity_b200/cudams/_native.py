@@ -67,6 +67,7 @@ SIGNATURES = {
         _p, _p, _p, _p, _p, c_int64, _p, _p]),
     "cms_library_destroy": (c_int, [_p]),
     "cms_profile_enable": (c_int, [_p, c_int]),
+    "cms_trace_enable": (c_int, [_p, _p, c_int64, _p, c_uint32]),
     "cms_graph_enable": (c_int, [_p, c_int]),
     "cms_profile_read": (c_int, [_p, _p, _p, c_int]),
     "cms_fingerprint": (c_int, [
@@ -95,7 +96,19 @@ class CosineConfig(ctypes.Structure):
         ("pair_threads", c_int32),
         ("cand_per_pair", c_double),
         ("symmetric", c_int32),
+        ("width_by_class", c_int32 * 17),
     ]
+
+    @classmethod
+    def from_dict(cls, config: dict) -> "CosineConfig":
+        c = cls()
+        for k, v in config.items():
+            if k == "width_by_class":
+                w = [int(x) for x in v][:17]
+                c.width_by_class = (c_int32 * 17)(*(w + [0] * (17 - len(w))))
+            else:
+                setattr(c, k, v)
+        return c
 
 
 _lib = None
@@ -153,6 +166,17 @@ class Context:
         """Capture repeated identical cms_cosine_greedy(_sparse) calls of this
         context into CUDA graphs and replay them (cms_graph_enable)."""
         check(load().cms_graph_enable(self.handle, 1 if on else 0), "cms_graph_enable")
+
+    def trace_enable(self, records, count, tag: int) -> None:
+        """Record every join work item of this context into `records` (device
+        int64 tensor [cap, 4]: tag | SM id << 32, item, start ns, end ns);
+        `count` (device int64 [1]) is advanced per record (cms_trace_enable)."""
+        check(load().cms_trace_enable(self.handle, c_void_p(records.data_ptr()),
+                                      int(records.shape[0]), c_void_p(count.data_ptr()),
+                                      int(tag) & 0xFFFFFFFF), "cms_trace_enable")
+
+    def trace_disable(self) -> None:
+        check(load().cms_trace_enable(self.handle, None, 0, None, 0), "cms_trace_enable")
 
     def profile_enable(self, on: bool = True) -> None:
         check(load().cms_profile_enable(self.handle, 1 if on else 0), "cms_profile_enable")

@@ -19,10 +19,7 @@ from .packing import DeviceSpectra
 def _cfg(config: Optional[dict]):
     if not config:
         return None
-    c = CosineConfig()
-    for k, v in config.items():
-        setattr(c, k, v)
-    return c
+    return CosineConfig.from_dict(config)
 
 
 def _stream(device, stream):

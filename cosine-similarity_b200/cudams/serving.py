@@ -79,9 +79,7 @@ class SpectrumLibrary:
         if "cand_per_pair" not in cfg:
             cfg["cand_per_pair"] = autotune.workload_stats(packed, packed, tolerance,
                                                            shift).cand_per_pair
-        c = CosineConfig()
-        for k, v in cfg.items():
-            setattr(c, k, v)
+        c = CosineConfig.from_dict(cfg)
         self.config = cfg
         ctx = _native.context(self.device.index)
         h = ctypes.c_void_p()

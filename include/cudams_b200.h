@@ -108,6 +108,19 @@ int cms_profile_enable(cms_ctx* ctx, int enable);
 int cms_profile_read(cms_ctx* ctx, double* stage_ms, int64_t* stage_launches, int reset);
 
 /*
+ * Work-item trace of the join kernel, for tests and studies of scheduling
+ * (no reference counterpart).  While enabled on a context, every join launch
+ * of that context (cms_cosine_greedy*, cms_library_search) appends one record
+ * per work item (a spectrum of the sweeping side against one indexed tile)
+ * to `records` (device, 4 uint64 each): tag | (SM id << 32), the item index,
+ * and the device's %globaltimer (ns) when the item started and ended.
+ * *count (device) is advanced atomically and may exceed `capacity` (records
+ * beyond it are dropped); the caller zeroes it.  records == NULL disables.
+ */
+int cms_trace_enable(cms_ctx* ctx, uint64_t* records, int64_t capacity, uint64_t* count,
+                     uint32_t tag);
+
+/*
  * Plain greedy cosine: one (reference, query) pair per thread, the
  * reference's own kernel design restated in CUDA C++ for sm_100a -- 512
  * query threads per block over one reference spectrum, per-thread candidate
@@ -136,6 +149,10 @@ int cms_cosine_greedy_plain(const float* ref_mz, const double* ref_a, const doub
  *   cand_per_pair  expected candidates per pair (e.g. sampled on the host);
  *                  sizes the first query sub-range of large spectra so the
  *                  join's candidate pool rarely overflows (0: unknown)
+ *   width_by_class first query sub-range width (queries swept per pool fill)
+ *                  for reference spectra of length class c = bit length of
+ *                  the peak count (c = 0..16); 0: derived from cand_per_pair.
+ *                  Set by cudams.autotune from timed trials per class.
  * One field changes the result rather than the speed:
  *   symmetric      nonzero: matchms' is_symmetric=True (matchms
  *                  BaseSimilarity.matrix; accepted but ignored by the
@@ -153,6 +170,7 @@ typedef struct {
     int32_t pair_threads;
     double cand_per_pair;
     int32_t symmetric;
+    int32_t width_by_class[17];
 } cms_cosine_config;
 
 /*
@@ -211,7 +229,11 @@ int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* re
  * `stream`) and freed by cms_library_destroy.  cfg (may be NULL) sets the
  * library tile size / bucket width and the expected candidates per pair.
  * Searches on different contexts and streams may run concurrently against
- * one library (it is read-only after creation).  Hit buffers and hit_count
+ * one library (it is read-only after creation).  A search launches
+ * short-lived CTAs (each warp takes a few work items and exits), so that the
+ * SMs free up continuously and searches on other streams -- give urgent ones
+ * a higher stream priority -- are scheduled in between: concurrent searches
+ * overlap on the device.  Hit buffers and hit_count
  * follow cms_cosine_greedy_sparse (hit_ref = library index, hit_query =
  * query index).
  */

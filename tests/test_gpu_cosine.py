@@ -62,6 +62,22 @@ def test_lognormal_heavy_tail(cuda_device):
     assert_same(gpu_dense(ref, qry, p, {"mode": 1, "tile_spectra": 4096}), want, "tile4096")
 
 
+def test_per_class_widths(cuda_device):
+    """Per-length-class first sub-range widths (the tuner's per-bucket choice):
+    narrow, odd and whole-tile widths for different classes, results
+    bit-exact."""
+    from cudams import synthetic
+
+    ref = synthetic.lognormal_spectra(900, seed=13)
+    qry = synthetic.lognormal_spectra(1100, seed=14)
+    p = P(0.01, 4096)
+    want = oracle.cosine_greedy(ref, qry, 0.01, 0.0, 4096)
+    widths = [0] * 17
+    widths[5], widths[6], widths[7], widths[8], widths[9], widths[10] = 32, 1, 96, 1024, 64, 7
+    assert_same(gpu_dense(ref, qry, p, {"mode": 1, "tile_spectra": 1024,
+                                        "width_by_class": widths}), want, "widths")
+
+
 def test_clustered_overflow(cuda_device):
     """Overflow-stress distribution: ~all pairs reach match_limit; flags and counts exact."""
     from cudams import synthetic

@@ -57,12 +57,23 @@ def test_cosine_config_layout_matches_the_header():
     from cudams._native import CosineConfig
 
     want = {"tile_spectra": 0, "bucket_width": 8, "n_buckets": 16, "mode": 20,
-            "pair_threads": 24, "cand_per_pair": 32, "symmetric": 40}
+            "pair_threads": 24, "cand_per_pair": 32, "symmetric": 40, "width_by_class": 44}
     got = {name: getattr(CosineConfig, name).offset for name, _ in CosineConfig._fields_}
     assert got == want
-    assert ctypes.sizeof(CosineConfig) == 48
+    assert ctypes.sizeof(CosineConfig) == 112
     header = (ROOT / "include" / "cudams_b200.h").read_text()
     body = header[header.index("typedef struct {", header.index("Tuning of the tiled path")):
                   header.index("} cms_cosine_config;")]
-    assert [ln.split()[-1].rstrip(";") for ln in body.splitlines()[1:] if ln.strip()] == \
-        list(want)
+    names = [ln.split()[-1].rstrip(";") for ln in body.splitlines()[1:] if ln.strip()]
+    assert [n.split("[")[0] for n in names] == list(want)
+    assert names[-1] == "width_by_class[17]"
+
+
+def test_cosine_config_from_dict():
+    """Per-class widths (a list, as the tuner's JSON cache holds them) fill the
+    17-entry array, zero-padded; other keys map to fields."""
+    from cudams._native import CosineConfig
+
+    c = CosineConfig.from_dict({"mode": 1, "tile_spectra": 640, "width_by_class": [0, 0, 32, 64]})
+    assert c.mode == 1 and c.tile_spectra == 640
+    assert list(c.width_by_class) == [0, 0, 32, 64] + [0] * 13
