@@ -61,6 +61,416 @@ __device__ __forceinline__ float measure_of(int inter, int a, int b) {
     return v != v ? 0.0f : v;
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core path: I = R . Q^T on tcgen05 (kind::i8, exact int32 in TMEM)
+// ---------------------------------------------------------------------------
+// The bit-packed rows are expanded to 0/1 bytes on the fly, straight into the
+// shared-memory operand stages (no expanded copy in global memory): a 0/1
+// byte dot product over K = n_words * 32 is exactly the intersection count.
+// The K order inside a 32-bit word is permuted by the expansion -- byte j of
+// output word v_s holds bit 8j + s -- identically for both operands, which
+// leaves every dot product unchanged.
+//
+// One persistent CTA per SM, warp-specialised:
+//   warps 0-7   epilogue: TMEM -> registers (tcgen05.ld 32x32b), measure in
+//               IEEE float32, 16-byte streaming stores (a lane writes 32
+//               consecutive floats of its row).  Warps w and w+4 share TMEM
+//               lanes 32*(w%4)..+31 (rows) and split the 256 columns.
+//   warps 8-11  producers: per 128-bit K block, load 16 bytes of each of the
+//               tile's 128 reference and 256 query rows, expand to 128 bytes
+//               each in the canonical K-major SWIZZLE_128B layout, make the
+//               writes visible to the tensor core (fence.proxy.async), and
+//               count the rows' bits (popcounts of the whole row per tile).
+//   warp 12     MMA issuer: one thread issues 4 x tcgen05.mma (M=128, N=256,
+//               K=32) per stage and commits stage release / accumulator ready.
+// Two 128 x 256 int32 accumulators (all 512 TMEM columns): the epilogue of
+// one tile overlaps the MMAs of the next.  Every mbarrier wait is bounded in
+// time; on expiry the kernel sets an error bit, every role stops, and TMEM is
+// released before exit.
+namespace umma {
+
+constexpr int kBM = 128;           // reference rows per tile (TMEM lanes)
+constexpr int kBN = 256;           // query rows per tile (accumulator columns)
+constexpr int kBKBytes = 128;      // expanded K bytes per stage (one 128B swizzle row)
+constexpr int kBKWords = kBKBytes / 32;  // packed uint32 words per row per stage
+constexpr int kStages = 4;
+constexpr int kABytes = kBM * kBKBytes;  // 16 KB
+constexpr int kBBytes = kBN * kBKBytes;  // 32 KB
+constexpr int kStageBytes = kABytes + kBBytes;
+constexpr int kEpiWarps = 8;
+constexpr int kProdWarps = 4;
+constexpr int kThreads = (kEpiWarps + kProdWarps + 1) * 32;
+constexpr int kProdThreads = kProdWarps * 32;
+constexpr int kTmemCols = 512;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
+
+// shared-memory layout (offsets from a 1024-byte aligned base)
+constexpr int kOffStages = 0;
+constexpr int kOffPop = kStages * kStageBytes;  // int pa[2][128], pb[2][256]
+constexpr int kOffBar = kOffPop + 2 * (kBM + kBN) * 4;
+// barriers: full[S], empty[S], tfull[2], tempty[2], pfull[2], pempty[2], done
+constexpr int kNumBars = 2 * kStages + 9;
+constexpr int kOffTmemSlot = kOffBar + kNumBars * 8;
+constexpr int kOffAbort = kOffTmemSlot + 4;
+constexpr int kSmemBytes = kOffAbort + 4 + 1024;  // + alignment slack
+
+// UMMA instruction descriptor: D s32, A/B u8, both K-major, M=128, N=256
+constexpr uint32_t kIdesc = (2u << 4) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of `parity` to complete, for at most kWaitNs; on expiry
+// (or, unless `drain`, when another role already gave up) raise the CTA's
+// abort flag and return false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          bool drain = false) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (!drain && *abort_flag) return false;
+        if (globaltimer() - t0 > kWaitNs) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// SWIZZLE_128B K-major shared-memory matrix descriptor (8-row atoms of
+// 128-byte rows, atoms 1024 bytes apart; Blackwell descriptor version 1)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) |
+           ((uint64_t)(1024u >> 4) << 32) | ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct Geometry {
+    int n_tm, n_tn;       // tiles along the reference / query side
+    int64_t n_tiles;
+    int kb;               // K blocks of kBKWords packed words (>= 1)
+};
+
+// Tile t -> (tm, tn); under `sym`, tiles wholly below the diagonal are skipped
+// by every role alike.
+__device__ __forceinline__ bool tile_live(const FpParams& P, const Geometry& G, int64_t t, int& tm,
+                                          int& tn) {
+    tm = (int)(t / G.n_tn);
+    tn = (int)(t - (int64_t)tm * G.n_tn);
+    if (!P.sym) return true;
+    return (int64_t)tm * kBM <= (int64_t)tn * kBN + (kBN - 1);
+}
+
+// 16 packed bytes (4 words) of one row's K block kb, zero beyond the matrix
+__device__ __forceinline__ uint4 load_bits(const uint32_t* base, int64_t row, int64_t n_rows,
+                                           int n_words, int kb, bool vec) {
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (row >= n_rows) return v;
+    const uint32_t* p = base + row * (int64_t)n_words + kb * kBKWords;
+    const int w0 = kb * kBKWords;
+    if (vec && w0 + kBKWords <= n_words) return __ldg(reinterpret_cast<const uint4*>(p));
+    if (w0 + 0 < n_words) v.x = __ldg(p + 0);
+    if (w0 + 1 < n_words) v.y = __ldg(p + 1);
+    if (w0 + 2 < n_words) v.z = __ldg(p + 2);
+    if (w0 + 3 < n_words) v.w = __ldg(p + 3);
+    return v;
+}
+
+// Expand one row's 128 bits into 128 bytes of 0/1 at row r of an operand
+// stage (SWIZZLE_128B: 16-byte chunk c of row r sits at chunk c ^ (r % 8)).
+__device__ __forceinline__ void expand_row(unsigned char* stage, int r, uint4 bits) {
+    unsigned char* row = stage + (r >> 3) * 1024 + (r & 7) * 128;
+    const uint32_t w[4] = {bits.x, bits.y, bits.z, bits.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t v[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) v[s] = (w[q] >> s) & 0x01010101u;
+        *reinterpret_cast<uint4*>(row + (((2 * q) ^ (r & 7)) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4*>(row + (((2 * q + 1) ^ (r & 7)) << 4)) =
+            make_uint4(v[4], v[5], v[6], v[7]);
+    }
+}
+
+template <int MEASURE>
+__global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geometry G,
+                                                               uint32_t* err) {
+    extern __shared__ unsigned char smem_dyn[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kOffBar);
+    uint64_t* full = bars;                    // [kStages] producers -> MMA
+    uint64_t* empty = bars + kStages;         // [kStages] MMA -> producers
+    uint64_t* tfull = bars + 2 * kStages;     // [2] MMA -> epilogue
+    uint64_t* tempty = tfull + 2;             // [2] epilogue -> MMA
+    uint64_t* pfull = tempty + 2;             // [2] producers -> epilogue (popcounts)
+    uint64_t* pempty = pfull + 2;             // [2] epilogue -> producers
+    uint64_t* done = pempty + 2;              // MMA completion before TMEM release
+    int* pa = reinterpret_cast<int*>(sm + kOffPop);  // [2][kBM]
+    int* pb = pa + 2 * kBM;                          // [2][kBN]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kOffTmemSlot);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kOffAbort);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], kProdThreads);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], kEpiWarps * 32);
+            mbar_init(&pfull[a], kProdThreads);
+            mbar_init(&pempty[a], kEpiWarps * 32);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {  // TMEM: all 512 columns, two accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp >= kEpiWarps && warp < kEpiWarps + kProdWarps) {
+        // ------------------------------ producers ------------------------------
+        const int pt = threadIdx.x - kEpiWarps * 32;  // 0..127
+        const bool vec = (P.n_words % kBKWords) == 0 &&
+                         (reinterpret_cast<uintptr_t>(P.r) & 15) == 0 &&
+                         (reinterpret_cast<uintptr_t>(P.q) & 15) == 0;
+        int stage = 0;
+        uint32_t phase = 0;
+        int64_t it = 0;  // tiles taken by this CTA
+        bool ok = true;
+        for (int64_t t = blockIdx.x; t < G.n_tiles && ok; t += gridDim.x) {
+            int tm, tn;
+            if (!tile_live(P, G, t, tm, tn)) continue;
+            const int acc = (int)(it & 1);
+            const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+            ++it;
+            const int64_t ra = (int64_t)tm * kBM + pt;
+            const int64_t qb0 = (int64_t)tn * kBN + pt, qb1 = qb0 + 128;
+            int ca = 0, cb0 = 0, cb1 = 0;
+            uint4 xa = load_bits(P.r, ra, P.n_r, P.n_words, 0, vec);
+            uint4 xb0 = load_bits(P.q, qb0, P.n_q, P.n_words, 0, vec);
+            uint4 xb1 = load_bits(P.q, qb1, P.n_q, P.n_words, 0, vec);
+            for (int kb = 0; kb < G.kb; ++kb) {
+                const uint4 a = xa, b0 = xb0, b1 = xb1;
+                if (kb + 1 < G.kb) {  // next block's bits load while this one expands
+                    xa = load_bits(P.r, ra, P.n_r, P.n_words, kb + 1, vec);
+                    xb0 = load_bits(P.q, qb0, P.n_q, P.n_words, kb + 1, vec);
+                    xb1 = load_bits(P.q, qb1, P.n_q, P.n_words, kb + 1, vec);
+                }
+                if (!mbar_wait(&empty[stage], phase ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char* sa = sm + kOffStages + stage * kStageBytes;
+                unsigned char* sb = sa + kABytes;
+                expand_row(sa, pt, a);
+                expand_row(sb, pt, b0);
+                expand_row(sb, pt + 128, b1);
+                ca += __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w);
+                cb0 += __popc(b0.x) + __popc(b0.y) + __popc(b0.z) + __popc(b0.w);
+                cb1 += __popc(b1.x) + __popc(b1.y) + __popc(b1.z) + __popc(b1.w);
+                fence_proxy_async_smem();
+                mbar_arrive(&full[stage]);
+                if (++stage == kStages) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+            if (!ok) break;
+            // the tile's row popcounts (-1: no fingerprint) for its epilogue
+            if (!mbar_wait(&pempty[acc], acc_phase ^ 1u, abort_flag)) break;
+            const bool va = ra < P.n_r && (P.r_valid ? P.r_valid[ra] != 0 : true);
+            const bool vb0 = qb0 < P.n_q && (P.q_valid ? P.q_valid[qb0] != 0 : true);
+            const bool vb1 = qb1 < P.n_q && (P.q_valid ? P.q_valid[qb1] != 0 : true);
+            pa[acc * kBM + pt] = va ? ca : -1;
+            pb[acc * kBN + pt] = vb0 ? cb0 : -1;
+            pb[acc * kBN + pt + 128] = vb1 ? cb1 : -1;
+            mbar_arrive(&pfull[acc]);
+        }
+    } else if (warp == kEpiWarps + kProdWarps) {
+        // ------------------------------ MMA issuer ------------------------------
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t it = 0;
+            bool ok = true;
+            for (int64_t t = blockIdx.x; t < G.n_tiles && ok; t += gridDim.x) {
+                int tm, tn;
+                if (!tile_live(P, G, t, tm, tn)) continue;
+                const int acc = (int)(it & 1);
+                const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+                ++it;
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1u, abort_flag)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(acc * kBN);
+                for (int kb = 0; kb < G.kb; ++kb) {
+                    if (!mbar_wait(&full[stage], phase, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(sm + kOffStages + stage * kStageBytes);
+                    const uint32_t sb = sa + kABytes;
+#pragma unroll
+                    for (int k = 0; k < kBKBytes / 32; ++k)
+                        umma_i8(d, smem_desc(sa + 32 * k), smem_desc(sb + 32 * k),
+                                (kb > 0 || k > 0) ? 1u : 0u);
+                    umma_commit(&empty[stage]);  // stage free once these MMAs have read it
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(&tfull[acc]);  // accumulator ready
+            }
+            // every MMA issued by this thread completes before TMEM is released
+            umma_commit(done);
+            mbar_wait(done, 0, abort_flag, true);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------ epilogue ------------------------------
+        const int quarter = warp & 3;        // TMEM lanes 32*quarter .. +31
+        const int half = warp >> 2;          // columns 128*half .. +127
+        const bool vec_out = (P.ld & 3) == 0 && (reinterpret_cast<uintptr_t>(P.out) & 15) == 0;
+        int64_t it = 0;
+        for (int64_t t = blockIdx.x; t < G.n_tiles; t += gridDim.x) {
+            int tm, tn;
+            if (!tile_live(P, G, t, tm, tn)) continue;
+            const int acc = (int)(it & 1);
+            const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+            ++it;
+            if (!mbar_wait(&tfull[acc], acc_phase, abort_flag)) break;
+            tc_fence_after();
+            if (!mbar_wait(&pfull[acc], acc_phase, abort_flag)) break;
+            const int row_l = quarter * 32 + lane;
+            const int a_cnt = pa[acc * kBM + row_l];
+            const int64_t gr = (int64_t)tm * kBM + row_l;  // this lane's output row
+            float* orow = P.out + gr * P.ld;
+            for (int c = 0; c < 4; ++c) {
+                const int col_l = half * 128 + c * 32;  // first column of this chunk in the tile
+                const int64_t gc0 = (int64_t)tn * kBN + col_l;
+                uint32_t v[32];
+                __syncwarp();
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kBN + col_l), v);
+                if (gr < P.n_r && gc0 < P.n_q) {
+                    float o[32];
+                    const int4* pbv = reinterpret_cast<const int4*>(pb + acc * kBN + col_l);
+#pragma unroll
+                    for (int j4 = 0; j4 < 8; ++j4) {
+                        const int4 b4 = pbv[j4];
+                        const int bc[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int j = 4 * j4 + u;
+                            o[j] = (a_cnt >= 0 && bc[u] >= 0)
+                                       ? measure_of<MEASURE>((int)v[j], a_cnt, bc[u])
+                                       : P.fill;
+                        }
+                    }
+                    // a lane writes 32 consecutive floats of its row: eight
+                    // 16-byte streaming stores when the chunk is whole, aligned
+                    // and (under sym) on or above the diagonal, else one by one
+                    if (vec_out && gc0 + 32 <= P.n_q && !(P.sym && gr > gc0)) {
+#pragma unroll
+                        for (int j4 = 0; j4 < 8; ++j4)
+                            __stcs(reinterpret_cast<float4*>(orow + gc0) + j4,
+                                   make_float4(o[4 * j4], o[4 * j4 + 1], o[4 * j4 + 2],
+                                               o[4 * j4 + 3]));
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int64_t gc = gc0 + j;
+                            if (gc < P.n_q && !(P.sym && gr > gc)) __stcs(orow + gc, o[j]);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);
+            mbar_arrive(&pempty[acc]);
+        }
+    }
+
+    __syncthreads();
+    if (*abort_flag && threadIdx.x == 0) atomicOr(err, 1u);
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+    }
+}
+
+}  // namespace umma
+
 template <int MEASURE>
 __global__ void __launch_bounds__(kFpThreads)
 fingerprint_kernel(FpParams P) {
@@ -150,6 +560,20 @@ fingerprint_kernel(FpParams P) {
     }
 }
 
+// Error bits of the tensor-core kernel (a pipeline wait that ran out of
+// time); read and cleared by cms_fingerprint_take_error.
+__device__ uint32_t g_fp_error;
+
+template <int MEASURE>
+int launch_umma(int grid, cudaStream_t s, const FpParams& P, const umma::Geometry& G,
+                uint32_t* err) {
+    auto* k = umma::fp_umma_kernel<MEASURE>;
+    if (const int rc = raise_func_smem(reinterpret_cast<const void*>(k), umma::kSmemBytes))
+        return rc;
+    k<<<grid, umma::kThreads, umma::kSmemBytes, s>>>(P, G, err);
+    return CMS_OK;
+}
+
 template <int MEASURE>
 int launch_fp(dim3 grid, size_t smem, cudaStream_t s, const FpParams& P) {
     if (const int rc = raise_func_smem(reinterpret_cast<const void*>(fingerprint_kernel<MEASURE>),
@@ -182,35 +606,34 @@ int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
         set_error("%s: null pointer", who);
         return CMS_ERR_INVALID;
     }
-    const int64_t gy = (n_ref + kBM - 1) / kBM, gx = (n_q + kBN - 1) / kBN;
-    if (gy > 65535 || gx > 2147483647LL) {
-        set_error("%s: too many rows for one launch (split the reference side)", who);
-        return CMS_ERR_UNSUPPORTED;
-    }
     FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld, sym};
-    dim3 grid((unsigned)gx, (unsigned)gy);
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = (size_t)(kBM + kBN) * kLd * sizeof(uint64_t);
+    int dev = 0, sms = 148;
+    CMS_CUDA_TRY(cudaGetDevice(&dev));
+    CMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    umma::Geometry G;
+    G.n_tm = (int)((n_ref + umma::kBM - 1) / umma::kBM);
+    G.n_tn = (int)((n_q + umma::kBN - 1) / umma::kBN);
+    G.n_tiles = (int64_t)G.n_tm * G.n_tn;
+    G.kb = std::max(1, (n_words + umma::kBKWords - 1) / umma::kBKWords);
+    uint32_t* err = nullptr;
+    CMS_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&err), g_fp_error));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sms, G.n_tiles));
     int rc = CMS_OK;
     switch (measure) {
         case CMS_FP_JACCARD:
-            rc = launch_fp<CMS_FP_JACCARD>(grid, smem, s, P);
+            rc = launch_umma<CMS_FP_JACCARD>(grid, s, P, G, err);
             break;
         case CMS_FP_DICE:
-            rc = launch_fp<CMS_FP_DICE>(grid, smem, s, P);
+            rc = launch_umma<CMS_FP_DICE>(grid, s, P, G, err);
             break;
         default:
-            rc = launch_fp<CMS_FP_COSINE>(grid, smem, s, P);
+            rc = launch_umma<CMS_FP_COSINE>(grid, s, P, G, err);
             break;
     }
     if (rc) return rc;
     CMS_CUDA_TRY(cudaGetLastError());
-    if (sym) {
-        int dev = 0, sms = 148;
-        CMS_CUDA_TRY(cudaGetDevice(&dev));
-        CMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        return launch_mirror(DenseOut{out, nullptr, nullptr, ld}, n_ref, nullptr, sms, s);
-    }
+    if (sym) return launch_mirror(DenseOut{out, nullptr, nullptr, ld}, n_ref, nullptr, sms, s);
     return CMS_OK;
 }
 
@@ -231,4 +654,20 @@ extern "C" int cms_fingerprint_symmetric(int measure, const uint32_t* ref_bits,
                                          float fill, float* out, int64_t ld, void* stream) {
     return cms::fingerprint_impl("cms_fingerprint_symmetric", measure, ref_bits, ref_valid, n,
                                  q_bits, q_valid, n, n_words, fill, out, ld, 1, stream);
+}
+
+extern "C" int cms_fingerprint_take_error(uint32_t* bits, void* stream) {
+    using namespace cms;
+    if (!bits) {
+        set_error("cms_fingerprint_take_error: null argument");
+        return CMS_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    uint32_t h = 0;
+    const uint32_t zero = 0;
+    CMS_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h, g_fp_error, sizeof(h), 0, cudaMemcpyDeviceToHost, s));
+    CMS_CUDA_TRY(cudaMemcpyToSymbolAsync(g_fp_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s));
+    CMS_CUDA_TRY(cudaStreamSynchronize(s));
+    *bits = h;
+    return CMS_OK;
 }

@@ -7,6 +7,7 @@ reported bad input through the context's error word.
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Optional
 
 import torch
@@ -166,12 +167,36 @@ def cosine_greedy_sparse(ref: DeviceSpectra, qry: DeviceSpectra, tolerance: floa
         cap = n
 
 
+def fingerprint_error(stream=None, device=None) -> int:
+    """Read and clear the fingerprint kernels' error bits (synchronises)."""
+    lib = _native.load()
+    s = _stream(device or torch.device("cuda", torch.cuda.current_device()), stream)
+    bits = ctypes.c_uint32(0)
+    check(lib.cms_fingerprint_take_error(ctypes.byref(bits), stream_handle(s)),
+          "cms_fingerprint_take_error")
+    return int(bits.value)
+
+
 def fingerprint_matrix(measure: str, r_bits, r_valid, q_bits, q_valid, n_words: int, fill: float,
-                       *, out=None, stream=None, symmetric: bool = False):
+                       *, out=None, stream=None, symmetric: bool = False,
+                       check_errors: bool = False):
     """Fingerprint similarity [n_ref, n_q] float32 on the device.
 
     symmetric: n_ref == n_q; only pairs (i, j) with i <= j are computed and
-    (j, i) gets the same value (matchms is_symmetric=True)."""
+    (j, i) gets the same value (matchms is_symmetric=True).
+    check_errors: synchronise and raise NativeError if a kernel reported a
+    pipeline timeout."""
+    out = _fingerprint_matrix(measure, r_bits, r_valid, q_bits, q_valid, n_words, fill, out=out,
+                              stream=stream, symmetric=symmetric)
+    if check_errors:
+        bits = fingerprint_error(stream, r_bits.device)
+        if bits:
+            raise _native.NativeError(f"fingerprint kernel error bits {bits:#x} (pipeline timeout)")
+    return out
+
+
+def _fingerprint_matrix(measure: str, r_bits, r_valid, q_bits, q_valid, n_words: int, fill: float,
+                        *, out=None, stream=None, symmetric: bool = False):
     lib = _native.load()
     device = r_bits.device
     s = _stream(device, stream)

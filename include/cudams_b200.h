@@ -289,7 +289,10 @@ int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a, const do
 
 /*
  * Fingerprint similarity on bit-packed fingerprints: n_words uint32 per
- * row, bit k in word k/32 at bit k%32, unused high bits zero.  Writes
+ * row, bit k in word k/32 at bit k%32, unused high bits zero.  The
+ * intersection counts I = R . Q^T run on the tensor cores (tcgen05, 8-bit
+ * integer operands expanded from the bits in shared memory, exact int32
+ * accumulation).  Writes
  * out[i*ld + j] (float32) for every (reference i, query j):
  *   CMS_FP_JACCARD  I / (a + b - I)      vector_similarity_functions.py:42-46
  *   CMS_FP_DICE     2 * (I / (a + b))    vector_similarity_functions.py:87-90
@@ -303,6 +306,15 @@ int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a, const do
 int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
                     int64_t n_ref, const uint32_t* q_bits, const uint8_t* q_valid, int64_t n_q,
                     int n_words, float fill, float* out, int64_t ld, void* stream);
+
+/*
+ * Read and clear the error bits of the fingerprint kernels (synchronises
+ * `stream`; *bits is a host pointer).  No reference counterpart.  The
+ * fingerprint kernels run a multi-stage pipeline whose internal waits are
+ * bounded in time; a nonzero word means one ran out of time and the results
+ * of the calls since the last read are not valid.
+ */
+int cms_fingerprint_take_error(uint32_t* bits, void* stream);
 
 /*
  * cms_fingerprint with matchms' is_symmetric=True (the reference's

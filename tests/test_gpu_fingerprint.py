@@ -1,5 +1,6 @@
-"""Fingerprint popcount kernel vs the oracle and the reference's own float32
-formulas: bit-exact."""
+"""Fingerprint kernel (tensor-core intersection counts) vs the oracle and the
+reference's own float32 formulas: bit-exact.  Every call also checks the
+kernel's error word (a pipeline wait that ran out of time)."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,8 @@ def _gpu(measure, rb, rv, qb, qv, n_words, fill):
 
     dev = torch.device("cuda", torch.cuda.current_device())
     t = lambda x: None if x is None else torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa
-    out = kernels.fingerprint_matrix(measure, t(rb), t(rv), t(qb), t(qv), n_words, fill)
+    out = kernels.fingerprint_matrix(measure, t(rb), t(rv), t(qb), t(qv), n_words, fill,
+                                     check_errors=True)
     return out.cpu().numpy()
 
 
@@ -134,7 +136,7 @@ def test_symmetric(cuda_device, measure, n):
     vb[130] = 0
     full_aa = oracle.fingerprint(measure, a, va, a, va, n_words, np.nan)
     got = kernels.fingerprint_matrix(measure, t(a), t(va), t(a), t(va), n_words, np.nan,
-                                     symmetric=True).cpu().numpy()
+                                     symmetric=True, check_errors=True).cpu().numpy()
     _bits_equal(got, full_aa)
 
     full_ab = oracle.fingerprint(measure, a, va, b, vb, n_words, -1.0)
@@ -143,7 +145,7 @@ def test_symmetric(cuda_device, measure, n):
     want[lower] = full_ab.T[lower]
     assert (want != full_ab).any()
     got = kernels.fingerprint_matrix(measure, t(a), t(va), t(b), t(vb), n_words, -1.0,
-                                     symmetric=True).cpu().numpy()
+                                     symmetric=True, check_errors=True).cpu().numpy()
     _bits_equal(got, want)
 
 
