@@ -8,13 +8,17 @@ against it with sparse output (pairs with score >= threshold,
 cms_library_search), as the sparse branch of matrix() would return them.
 
 Server: requests (query batches of any size) are queued as they arrive.  Each
-of `slots` worker threads owns a CUDA stream and a library context; a worker
-takes the next request as soon as it is free and the request's estimated
-device memory fits in the free HBM (minus a reserve), so requests that
-arrive while others are on the GPU start immediately and their kernels run
-concurrently on separate streams (a small batch launches only the CTAs it can
-keep busy).  Every request's result depends only on its own queries: it is
-the same alone or in the mix.
+of `slots` worker threads owns a library context and two CUDA streams (high
+and low priority); a worker takes the next request as soon as it is free and
+the request's estimated device memory fits in the free HBM (minus a reserve),
+so requests that arrive while others are on the GPU start immediately.
+Their work overlaps on the device: a search launches short-lived CTAs (each
+warp takes a few work items and exits), so SM slots free up continuously and
+the CTAs of searches on other streams are scheduled in between; requests of
+at most `chunk` queries run on the high-priority stream, so their CTAs are
+dispatched ahead of the pending CTAs of larger batches (which run
+`chunk` queries at a time on the low-priority one).  Every request's result
+depends only on its own queries: it is the same alone or in the mix.
 """
 from __future__ import annotations
 
@@ -192,21 +196,29 @@ class _Request:
     future: Future
     t_submit: float
     est_bytes: int
+    seq: int = 0
 
 
 class Server:
     """Continuous-batching search server over one SpectrumLibrary."""
 
     def __init__(self, library: SpectrumLibrary, threshold: float = 0.7, slots: int = 4,
-                 reserve_bytes: int = 4 << 30, warmup_queries: int = 4096, chunk: int = 1024):
-        """slots: concurrent searches (one stream and context each).
+                 reserve_bytes: int = 4 << 30, warmup_queries: int = 4096, chunk: int = 1024,
+                 trace_capacity: int = 0):
+        """slots: concurrent searches (one context and stream pair each).
         warmup_queries: each slot first searches this many copies of a library
         spectrum, so that its device scratch and pinned staging are sized for
         the largest expected batch before requests arrive (allocations
-        synchronise the device and would otherwise land on request latency)."""
+        synchronise the device and would otherwise land on request latency).
+        trace_capacity > 0: every result carries extra["trace"], the device
+        timing records of its work items (cms_trace_enable; tag = request
+        number), for studies of how requests overlap on the device."""
         import torch
 
         self.library = library
+        self.trace_capacity = int(trace_capacity)
+        self._seq = 0
+        self._seq_lock = threading.Lock()
         self.warmup_queries = int(warmup_queries)
         self.chunk = int(chunk)
         self._ready = threading.Barrier(int(slots) + 1)
@@ -239,8 +251,11 @@ class Server:
         q = self.library.pack_queries(queries)
         f: Future = Future()
         cap = max(4096, 64 * max(1, q.n))
+        with self._seq_lock:
+            self._seq += 1
+            seq = self._seq
         self._q.put(_Request(q, self.threshold if threshold is None else float(threshold), f, t,
-                             self.library.estimate_bytes(q, cap)))
+                             self.library.estimate_bytes(q, cap), seq))
         return f
 
     def close(self):
@@ -296,9 +311,16 @@ class Server:
     def _worker(self):
         import torch
 
-        torch.cuda.set_device(self.library.device)
-        stream = torch.cuda.Stream(self.library.device)
+        urgent = stream = trace = None
         try:
+            torch.cuda.set_device(self.library.device)
+            # lower number = higher priority; out-of-range values are clamped
+            urgent = torch.cuda.Stream(self.library.device, priority=-5)
+            stream = torch.cuda.Stream(self.library.device, priority=0)
+            if self.trace_capacity > 0:
+                trace = (torch.zeros((self.trace_capacity, 4), dtype=torch.int64,
+                                     device=self.library.device),
+                         torch.zeros(1, dtype=torch.int64, device=self.library.device))
             if self.warmup_queries > 0:
                 one = self.library.packed.subset(0, 1)
                 k = self.warmup_queries
@@ -318,12 +340,24 @@ class Server:
             self._admit(req)
             t_start = time.perf_counter()
             try:
-                res = self.library.search(req.queries, req.threshold, stream=stream,
+                small = req.queries.n <= self.chunk
+                target = urgent if small else stream
+                if trace is not None:
+                    ctx = _native.context(self.library.device.index)
+                    with torch.cuda.stream(target):
+                        trace[1].zero_()
+                    ctx.trace_enable(trace[0], trace[1], req.seq)
+                res = self.library.search(req.queries, req.threshold, stream=target,
                                           chunk=self.chunk)
                 res.queued_s = t_start - req.t_submit
                 res.latency_s = time.perf_counter() - req.t_submit
                 res.extra.update(dequeue_s=t_deq - req.t_submit, admit_s=t_start - t_deq,
-                                 search_s=res.latency_s - res.queued_s)
+                                 search_s=res.latency_s - res.queued_s, seq=req.seq,
+                                 priority="high" if small else "low")
+                if trace is not None:
+                    ctx.trace_disable()
+                    n = min(int(trace[1].item()), self.trace_capacity)
+                    res.extra["trace"] = trace[0][:n].cpu().numpy()
                 req.future.set_result(res)
             except BaseException as e:  # noqa: BLE001 - forwarded to the caller
                 req.future.set_exception(e)

@@ -54,7 +54,7 @@ def fake_cuda(monkeypatch):
 
     budget = {"free": 10_000}
     monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
-    monkeypatch.setattr(torch.cuda, "Stream", lambda d=None: None)
+    monkeypatch.setattr(torch.cuda, "Stream", lambda d=None, priority=0: None)
     monkeypatch.setattr(torch.cuda, "mem_get_info", lambda d=None: (budget["free"], 1 << 40))
     return budget
 
