@@ -15,8 +15,18 @@ and a random query peak fall within the window (exact window counts of a
 seeded peak sample against a sorted sample of query peaks, with numpy),
 times the peaks per spectrum of each side.  Sampling whole pairs instead
 gives a noisy mean when peak counts are heavy-tailed; the pair sample is
-kept for the 99th percentile.  Tuned settings can be pinned per workload key
-in an on-disk cache (JSON) by `Tuner.record`.
+kept for the 99th percentile.  That estimate gives the starting point
+(`heuristic_config`).
+
+`Tuner.measure` then chooses by timed trials on the device (CUDA events, a
+sample of the workload): first the tile size among neighbours of the
+estimate, then, per peak-count bucket of the reference spectra (length
+class = bit length of the peak count), the width of the first query
+sub-range swept per candidate-pool fill (cms_cosine_config.width_by_class:
+narrower ranges keep a large spectrum's candidates in the shared-memory
+pool, wider ones amortise its bucket lookups over more queries).  The
+winners are recorded per workload key in an on-disk cache (JSON,
+`Tuner.record`) that `choose_config` consults first.
 """
 from __future__ import annotations
 
@@ -164,7 +174,104 @@ class Tuner:
                 pass
 
 
+    def measure(self, ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
+                shift: float = 0.0, match_limit: int = 2048, device=None, gpu: str = "B200",
+                sample_ref: int = 4096, sample_qry: int = 20000, reps: int = 3,
+                record: bool = True, seed: int = 0):
+        """Choose tile_spectra and width_by_class by timed trials on the device.
+
+        Returns (config, report); report lists every trial (ms per trial on
+        the sample) and the chosen setting per bucket."""
+        import time
+
+        import torch
+
+        from . import _native, kernels
+
+        dev = _native.require_cuda(device)
+        t_start = time.perf_counter()
+        stats = workload_stats(ref, qry, tolerance, shift)
+        base = heuristic_config(stats, qry.n, ref.n)
+        report = {"heuristic": dict(base), "trials": [], "buckets": {}}
+        if base["mode"] == 2 or ref.n == 0 or qry.n == 0:
+            report["seconds"] = time.perf_counter() - t_start
+            return base, report
+        rng = np.random.default_rng(seed)
+        qs = qry.subset(0, min(qry.n, sample_qry))
+        qd = qs.to_device(dev)
+        lengths = ref.lengths
+        classes = np.where(lengths > 0, np.floor(np.log2(np.maximum(lengths, 1))).astype(int) + 1, 0)
+        pick = np.sort(rng.choice(ref.n, min(ref.n, sample_ref), replace=False))
+        rs = ref.take(pick)
+        rd = rs.to_device(dev)
+        out = tuple(torch.empty((max(rs.n, 1024), qs.n), dtype=t, device=dev)
+                    for t in (torch.float32, torch.int32, torch.uint8))
+
+        def timed(rdev, n_rows, cfg):
+            o = tuple(t[:n_rows] for t in out)
+            run = lambda: kernels.cosine_greedy_dense(rdev, qd, tolerance, shift,  # noqa: E731
+                                                      match_limit, out=o, config=cfg)
+            run()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        # 1) tile size: the estimate and its neighbours
+        t0 = base["tile_spectra"]
+        tiles = sorted({max(32, min(4096, (t + 31) // 32 * 32)) for t in (t0 // 2, t0, 2 * t0)})
+        best_tile, best_ms = t0, float("inf")
+        for t in tiles:
+            ms = timed(rd, rs.n, dict(base, tile_spectra=t))
+            report["trials"].append({"tile_spectra": t, "ms": ms})
+            if ms < best_ms:
+                best_tile, best_ms = t, ms
+        tile = min(best_tile, max(32, qs.n))
+        # 2) first sub-range width per reference length class
+        widths = [0] * 17
+        for c in range(17):
+            members = np.nonzero(classes == c)[0]
+            if members.size < 16:
+                continue
+            sel = np.sort(rng.choice(members, min(members.size, 1024), replace=False))
+            sub = ref.take(sel)
+            sd = sub.to_device(dev)
+            options = [0] + sorted({max(32, (tile // d) // 32 * 32) for d in (1, 2, 4, 8)},
+                                   reverse=True)
+            res = []
+            for w in options:
+                wbc = [0] * 17
+                wbc[c] = w
+                ms = timed(sd, sub.n, dict(base, tile_spectra=tile, width_by_class=wbc))
+                res.append((ms, w))
+                report["trials"].append({"class": c, "width": w, "ms": ms})
+            ms0 = res[0][0]
+            ms_best, w_best = min(res)
+            # keep the estimate unless a width is measurably faster (>= 2%)
+            if w_best and ms_best < 0.98 * ms0:
+                widths[c] = w_best
+            report["buckets"][c] = {"spectra": int(members.size),
+                                    "peaks": [1 << max(c - 1, 0), (1 << c) - 1],
+                                    "width": widths[c], "ms_default": ms0,
+                                    "ms_chosen": min(ms0, ms_best) if widths[c] else ms0}
+        cfg = dict(base, tile_spectra=tile, width_by_class=widths)
+        report["seconds"] = time.perf_counter() - t_start
+        if record:
+            self.record(stats, gpu, cfg)
+        return cfg, report
+
+
 _default = Tuner()
+
+
+def measure(ref: PackedSpectra, qry: PackedSpectra, tolerance: float, shift: float = 0.0,
+            match_limit: int = 2048, device=None, gpu: str = "B200", **kw):
+    """Timed per-bucket tuning of the default tuner (see Tuner.measure)."""
+    return _default.measure(ref, qry, tolerance, shift, match_limit, device, gpu, **kw)
 
 
 def choose_config(ref: PackedSpectra, qry: PackedSpectra, tolerance: float, shift: float = 0.0,

@@ -120,6 +120,18 @@ class PackedSpectra:
                              off, self.mz_power, self.intensity_power, int(n_max_peaks),
                              _b32=None if self._b32 is None else self._b32[idx])
 
+    def take(self, indices) -> "PackedSpectra":
+        """The spectra at `indices` (in that order) as a new packed set."""
+        idx = np.asarray(indices, dtype=np.int64)
+        keep = self.lengths[idx]
+        off = np.zeros(idx.shape[0] + 1, dtype=np.int64)
+        np.cumsum(keep, out=off[1:])
+        seg = np.repeat(np.arange(idx.shape[0]), keep)
+        pk = self.offsets[:-1][idx][seg] + (np.arange(off[-1]) - off[:-1][seg])
+        return PackedSpectra(self.mz[pk], None if self.a is None else self.a[pk], self.b[pk],
+                             off, self.mz_power, self.intensity_power, self.n_max_peaks,
+                             _b32=None if self._b32 is None else self._b32[pk])
+
     def subset(self, start: int, stop: int) -> "PackedSpectra":
         """Spectra [start, stop) as a new packed set (peaks re-based to 0)."""
         lo, hi = int(self.offsets[start]), int(self.offsets[stop])

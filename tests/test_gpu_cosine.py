@@ -78,6 +78,23 @@ def test_per_class_widths(cuda_device):
                                         "width_by_class": widths}), want, "widths")
 
 
+def test_measured_tuner_config(cuda_device, tmp_path):
+    """Tuner.measure times tiles and per-bucket widths on the device, records
+    them, and the chosen config computes the oracle's results."""
+    from cudams import autotune, synthetic
+
+    ref = synthetic.lognormal_spectra(3000, seed=15)
+    qry = synthetic.lognormal_spectra(2500, seed=16)
+    t = autotune.Tuner(str(tmp_path / "tune.json"))
+    cfg, report = t.measure(ref, qry, 0.01, 0.0, 4096, sample_ref=1000, sample_qry=2500)
+    assert cfg["mode"] == 1 and len(cfg["width_by_class"]) == 17
+    assert report["trials"] and report["buckets"]
+    st = autotune.workload_stats(ref, qry, 0.01)
+    assert t.lookup(st, "B200", qry.n, ref.n) == cfg
+    want = oracle.cosine_greedy(ref, qry, 0.01, 0.0, 4096)
+    assert_same(gpu_dense(ref, qry, P(0.01, 4096), cfg), want, "measured")
+
+
 def test_clustered_overflow(cuda_device):
     """Overflow-stress distribution: ~all pairs reach match_limit; flags and counts exact."""
     from cudams import synthetic

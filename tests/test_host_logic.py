@@ -5,6 +5,8 @@ import json
 import sys
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -77,3 +79,33 @@ def test_cosine_config_from_dict():
     c = CosineConfig.from_dict({"mode": 1, "tile_spectra": 640, "width_by_class": [0, 0, 32, 64]})
     assert c.mode == 1 and c.tile_spectra == 640
     assert list(c.width_by_class) == [0, 0, 32, 64] + [0] * 13
+
+
+def test_tuner_records_per_bucket_widths(tmp_path):
+    """A measured config (per-bucket widths included) round-trips through the
+    on-disk cache and is what lookup returns for that workload's bucket."""
+    from cudams import autotune
+
+    t = autotune.Tuner(str(tmp_path / "tune.json"))
+    st = autotune.WorkloadStats(0.1, 2.0, 99.0, 99.0)
+    cfg = {"mode": 1, "tile_spectra": 1344, "cand_per_pair": 0.1,
+           "width_by_class": [0] * 8 + [320, 160] + [0] * 7}
+    t.record(st, "B200", cfg)
+    got = autotune.Tuner(str(tmp_path / "tune.json")).lookup(st, "B200", 100_000, 100_000)
+    assert got == cfg
+    key = autotune.Tuner.key(st, "B200")
+    assert key.startswith("B200|c") and "|r6|" in key and key.endswith("|q6")
+
+
+def test_take_selects_spectra():
+    from cudams import synthetic
+
+    P = synthetic.lognormal_spectra(50, seed=1)
+    idx = [5, 2, 49, 0, 5]
+    T = P.take(idx)
+    assert T.n == 5
+    for k, i in enumerate(idx):
+        np.testing.assert_array_equal(T.mz[T.offsets[k]:T.offsets[k + 1]],
+                                      P.mz[P.offsets[i]:P.offsets[i + 1]])
+        np.testing.assert_array_equal(T.b[T.offsets[k]:T.offsets[k + 1]],
+                                      P.b[P.offsets[i]:P.offsets[i + 1]])
