@@ -22,6 +22,12 @@ Workloads
                      n_max_peaks 2048)
   fingerprints       2048-bit fingerprints, per-fingerprint density
                      U(5%, 15%), bits iid, packed as uint32 words
+  analog_spectra     families of structural analogues for modified cosine:
+                     a base spectrum (lognormal peak count, m/z below the
+                     precursor) and members whose precursor and upper
+                     fragments move by one mass difference, with jitter,
+                     dropped and added peaks; returns the spectra and their
+                     precursor m/z
 """
 from __future__ import annotations
 
@@ -138,3 +144,44 @@ def fingerprints(n: int, n_bits: int = 2048, seed: int = 0, dmin: float = 0.05,
         packed = np.packbits(dense, axis=1, bitorder="little")
         out[s:e] = np.ascontiguousarray(packed).view("<u4").reshape(e - s, n_words)
     return out
+
+
+def analog_spectra(n: int, seed: int = 0, family_size: int = 8, n_max_peaks: int = 1024,
+                   mz_power: float = 0.0, intensity_power: float = 1.0, median_peaks: float = 60.0):
+    """(PackedSpectra, precursor_mz float64[n]): families of `family_size`
+    analogues.  Member k of a family shares the base spectrum's peaks; peaks
+    above a random cut move by the member's mass difference d (one in four
+    members has d = 0), every peak is jittered by N(0, 0.002^2), a tenth are
+    dropped and a few noise peaks are added; its precursor is the base
+    precursor + d."""
+    rng = np.random.default_rng(seed)
+    spectra, prec = [], np.empty(n, np.float64)
+    base = None
+    for i in range(n):
+        if i % family_size == 0:
+            k = int(np.clip(np.round(rng.lognormal(np.log(median_peaks), 0.6)), 5, 600))
+            p0 = rng.uniform(300.0, 1500.0)
+            bmz = np.sort(rng.uniform(50.0, p0 - 5.0, k))
+            bint = rng.exponential(1.0, k)
+            cut = rng.uniform(0.3, 0.8) * p0
+            base = (bmz, bint, p0, cut)
+        bmz, bint, p0, cut = base
+        d = 0.0 if rng.random() < 0.25 else float(rng.uniform(-40.0, 40.0))
+        keep = rng.random(bmz.shape[0]) >= 0.1
+        mz = np.where(bmz > cut, bmz + d, bmz)[keep] + rng.normal(0.0, 0.002, int(keep.sum()))
+        it = bint[keep] * rng.uniform(0.7, 1.3, int(keep.sum()))
+        extra = int(rng.integers(0, 6))
+        mz = np.concatenate([mz, rng.uniform(50.0, p0 + d, extra)])
+        it = np.concatenate([it, rng.exponential(0.3, extra)])
+        mz = np.clip(mz, 1.0, None)
+        order = np.argsort(mz, kind="stable")
+        spectra.append((mz[order], it[order] / max(it.max(), 1e-12)))
+        prec[i] = p0 + d
+    lengths = np.array([m.shape[0] for m, _ in spectra], np.int64)
+    mz = np.concatenate([m for m, _ in spectra]).astype(np.float32)
+    inten = np.concatenate([x for _, x in spectra])
+    off, seg = _segments(lengths)
+    mz = _sort_within(mz, seg)  # float32 rounding can reorder near-equal m/z
+    packed = pack_csr(mz, inten.astype(np.float32), off, n_max_peaks, mz_power, intensity_power,
+                      check=False)
+    return packed, prec

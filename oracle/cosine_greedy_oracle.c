@@ -44,6 +44,21 @@
  *   counts); an empty spectrum on either side gives (0, 0, 0) (:70, :100); no
  *   candidates gives score 0, matches 0 (:153).
  *
+ * Modified cosine (matchms ModifiedCosine, the published algorithm of the
+ *   same third-party package; the reference prototypes it beside its CUDA
+ *   classes, notebooks/prototyping/other_similarities.ipynb cells 5 and 8, and
+ *   carries the shift it needs into its kernel, spectrum_similarity_functions
+ *   .py:14,133): the candidates are the matches at shift 0 followed by the
+ *   matches at shift = precursor_mz(reference) - precursor_mz(query) (both
+ *   float64, the matchms metadata), each list generated as above (p1-major,
+ *   p2 ascending); keys, the stable descending sort over the concatenation
+ *   (ties -> later position first, so a shifted candidate precedes an
+ *   unshifted one of equal key), the greedy and the norms are those of mode 0.
+ *   matchms has no candidate limit; here, as for greedy cosine, generation
+ *   stops once match_limit candidates exist in the concatenated order and
+ *   overflow is set, so a match_limit above every pair's count gives matchms'
+ *   result exactly.
+ *
  * Fingerprints: cudams/similarity/vector_similarity_functions.py:42-46
  *   (jaccard I/(a+b-I)), :87-90 (dice 2*(I/(a+b))), :116-118 (cosine
  *   I/sqrt(a*b)), each in IEEE float32 with nan_to_num (0/0 -> 0).
@@ -100,6 +115,57 @@ static float norm2_f32(const double* a, const double* b, int64_t lo, int64_t hi)
         s = (float)((double)s + w * w);
     }
     return s;
+}
+
+/* Append the f64-mode candidates of one pair at `shift` (matchms find_matches
+ * + collect_peak_pairs) to cands[*n..]; returns 1 when match_limit is reached
+ * (overflow). */
+static int gen_f64(const float* rmz, const double* ra, const double* rb, int64_t r0, int64_t nr,
+                   const float* qmz, const double* qa, const double* qb, int64_t q0, int64_t nq,
+                   double tol, double shift, int match_limit, cand_t* cands, int* n) {
+    int64_t lowest = 0;
+    for (int64_t p1 = 0; p1 < nr; ++p1) {
+        double mz1 = (double)rmz[r0 + p1];
+        double lo = mz1 - tol, hi = mz1 + tol;
+        double w1 = peak_a(ra, r0 + p1) * rb[r0 + p1];
+        for (int64_t p2 = lowest; p2 < nq; ++p2) {
+            double mz2 = (double)qmz[q0 + p2] + shift;
+            if (mz2 > hi) break;
+            if (mz2 < lo) {
+                lowest = p2 + 1;
+                continue;
+            }
+            double key = (w1 * peak_a(qa, q0 + p2)) * qb[q0 + p2];
+            cands[*n].key = key;
+            cands[*n].gen = (uint32_t)*n;
+            cands[*n].p1 = (uint16_t)p1;
+            cands[*n].p2 = (uint16_t)p2;
+            if (++*n >= match_limit) return 1;
+        }
+    }
+    return 0;
+}
+
+/* greedy over sorted candidates; score and matches (f64 mode) */
+static void greedy_f64(cand_t* cands, int n, int64_t nr, int64_t nq, uint8_t* used_r,
+                       uint8_t* used_q, double n2r, double n2q, float* out_score,
+                       int32_t* out_matches) {
+    qsort(cands, (size_t)n, sizeof(cand_t), cand_cmp);
+    memset(used_r, 0, (size_t)nr);
+    memset(used_q, 0, (size_t)nq);
+    double score = 0.0;
+    int matches = 0;
+    for (int m = 0; m < n; ++m) {
+        int p1 = cands[m].p1, p2 = cands[m].p2;
+        if (!used_r[p1] && !used_q[p2]) {
+            used_r[p1] = 1;
+            used_q[p2] = 1;
+            score = score + cands[m].key;
+            ++matches;
+        }
+    }
+    *out_score = (float)(score / (sqrt(n2r) * sqrt(n2q)));
+    *out_matches = matches;
 }
 
 static void one_pair(const float* rmz, const double* ra, const double* rb, int64_t r0, int64_t nr,
@@ -250,6 +316,74 @@ int oracle_cosine_greedy(const float* rmz, const double* ra, const double* rb, c
     }
     free(n2r);
     free(n2q);
+    return failed ? -1 : 0;
+}
+
+/*
+ * Dense modified cosine over all (reference i, query j) pairs (f64 mode; see
+ * the header).  rprec / qprec: precursor m/z per spectrum.  Returns 0, or -1
+ * on bad arguments / allocation failure.
+ */
+int oracle_modified_cosine(const float* rmz, const double* ra, const double* rb,
+                           const int64_t* roff, const double* rprec, int64_t n_ref,
+                           const float* qmz, const double* qa, const double* qb,
+                           const int64_t* qoff, const double* qprec, int64_t n_q, double tol,
+                           int match_limit, float* out_score, int32_t* out_matches,
+                           uint8_t* out_overflow, int64_t ld, int n_threads) {
+    if (match_limit < 1 || ld < n_q) return -1;
+    int64_t max_nr = 0, max_nq = 0;
+    for (int64_t i = 0; i < n_ref; ++i)
+        if (roff[i + 1] - roff[i] > max_nr) max_nr = roff[i + 1] - roff[i];
+    for (int64_t j = 0; j < n_q; ++j)
+        if (qoff[j + 1] - qoff[j] > max_nq) max_nq = qoff[j + 1] - qoff[j];
+    if (max_nr > 65536 || max_nq > 65536) return -1;
+    int failed = 0;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel
+#endif
+    {
+        cand_t* cands = (cand_t*)malloc(sizeof(cand_t) * (size_t)match_limit);
+        uint8_t* used_r = (uint8_t*)malloc((size_t)max_nr + 1);
+        uint8_t* used_q = (uint8_t*)malloc((size_t)max_nq + 1);
+        if (!cands || !used_r || !used_q) {
+#ifdef _OPENMP
+#pragma omp atomic write
+#endif
+            failed = 1;
+        } else {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+            for (int64_t i = 0; i < n_ref; ++i) {
+                const int64_t r0 = roff[i], nr = roff[i + 1] - roff[i];
+                const double n2r = norm2_f64(ra, rb, roff[i], roff[i + 1]);
+                for (int64_t j = 0; j < n_q; ++j) {
+                    const int64_t o = i * ld + j;
+                    const int64_t q0 = qoff[j], nq = qoff[j + 1] - qoff[j];
+                    out_score[o] = 0.0f;
+                    out_matches[o] = 0;
+                    out_overflow[o] = 0;
+                    if (nr == 0 || nq == 0) continue;
+                    const double mass_shift = rprec[i] - qprec[j];
+                    int n = 0;
+                    int ovf = gen_f64(rmz, ra, rb, r0, nr, qmz, qa, qb, q0, nq, tol, 0.0,
+                                      match_limit, cands, &n);
+                    if (!ovf)
+                        ovf = gen_f64(rmz, ra, rb, r0, nr, qmz, qa, qb, q0, nq, tol, mass_shift,
+                                      match_limit, cands, &n);
+                    out_overflow[o] = (uint8_t)ovf;
+                    if (n == 0) continue;
+                    greedy_f64(cands, n, nr, nq, used_r, used_q, n2r,
+                               norm2_f64(qa, qb, qoff[j], qoff[j + 1]), &out_score[o],
+                               &out_matches[o]);
+                }
+            }
+        }
+        free(cands);
+        free(used_r);
+        free(used_q);
+    }
     return failed ? -1 : 0;
 }
 

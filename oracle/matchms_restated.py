@@ -75,3 +75,21 @@ def cosine_greedy_pair(mz1, int1, mz2, int2, tolerance=0.1, mz_power=0.0, intens
         return 0.0, 0
     pairs = pairs[np.argsort(pairs[:, 2], kind="mergesort")[::-1], :]
     return score_best_matches(pairs, spec1, spec2, mz_power, intensity_power)
+
+
+def modified_cosine_pair(mz1, int1, mz2, int2, precursor1, precursor2, tolerance=0.1,
+                         mz_power=0.0, intensity_power=1.0):
+    """(score float64, matches int) of one pair, matchms ModifiedCosine
+    semantics: the matches at shift 0 and at shift precursor1 - precursor2,
+    concatenated, sorted once (stable, reversed), then one greedy."""
+    spec1 = np.stack([np.asarray(mz1, np.float64), np.asarray(int1, np.float64)], axis=1)
+    spec2 = np.stack([np.asarray(mz2, np.float64), np.asarray(int2, np.float64)], axis=1)
+    zero = collect_peak_pairs(spec1, spec2, tolerance, 0.0, mz_power, intensity_power)
+    shifted = collect_peak_pairs(spec1, spec2, tolerance, float(precursor1) - float(precursor2),
+                                 mz_power, intensity_power)
+    parts = [x for x in (zero, shifted) if x is not None]
+    if not parts:
+        return 0.0, 0
+    pairs = np.concatenate(parts, axis=0)
+    pairs = pairs[np.argsort(pairs[:, 2], kind="mergesort")[::-1], :]
+    return score_best_matches(pairs, spec1, spec2, mz_power, intensity_power)

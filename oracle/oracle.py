@@ -38,6 +38,9 @@ def _load():
         lib.oracle_cosine_greedy_pairs.argtypes = [p, p, p, p, p, p, p, p, p, p, c_int64,
                                                    c_double, c_double, c_int, c_int, p, p, p,
                                                    c_int]
+        lib.oracle_modified_cosine.restype = c_int
+        lib.oracle_modified_cosine.argtypes = [p, p, p, p, p, c_int64, p, p, p, p, p, c_int64,
+                                               c_double, c_int, p, p, p, c_int64, c_int]
         lib.oracle_fingerprint.restype = c_int
         lib.oracle_fingerprint.argtypes = [c_int, p, p, c_int64, p, p, c_int64, c_int, c_float,
                                            p, c_int64, c_int]
@@ -77,6 +80,29 @@ def cosine_greedy(ref, qry, tolerance: float, shift: float, match_limit: int,
                                       int(threads))
     if rc != 0:
         raise RuntimeError("oracle_cosine_greedy failed")
+    return score, matches, overflow
+
+
+def modified_cosine(ref, qry, ref_precursor, qry_precursor, tolerance: float, match_limit: int,
+                    threads: int = 0):
+    """Dense modified cosine (score f32, matches i32, overflow u8) [n_ref, n_q]:
+    matchms ModifiedCosine restated (see cosine_greedy_oracle.c), float64."""
+    rm, ra, rb, ro = _side(ref)
+    qm, qa, qb, qo = _side(qry)
+    rp = np.ascontiguousarray(ref_precursor, dtype=np.float64)
+    qp = np.ascontiguousarray(qry_precursor, dtype=np.float64)
+    nr, nq = ro.shape[0] - 1, qo.shape[0] - 1
+    if rp.shape[0] != nr or qp.shape[0] != nq:
+        raise ValueError("one precursor m/z per spectrum")
+    score = np.zeros((nr, nq), np.float32)
+    matches = np.zeros((nr, nq), np.int32)
+    overflow = np.zeros((nr, nq), np.uint8)
+    rc = _load().oracle_modified_cosine(_ptr(rm), _ptr(ra), _ptr(rb), _ptr(ro), _ptr(rp), nr,
+                                        _ptr(qm), _ptr(qa), _ptr(qb), _ptr(qo), _ptr(qp), nq,
+                                        float(tolerance), int(match_limit), _ptr(score),
+                                        _ptr(matches), _ptr(overflow), nq, int(threads))
+    if rc != 0:
+        raise RuntimeError("oracle_modified_cosine failed")
     return score, matches, overflow
 
 

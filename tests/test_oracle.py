@@ -179,3 +179,39 @@ def test_fingerprint_oracle_bit_exact_vs_reference(name, measure):
         via_torch = np.nan_to_num(inter / t_sqrt, nan=0.0).astype(np.float32)
     np.testing.assert_array_equal(out[~quirk].view(np.uint32), ref[~quirk].view(np.uint32))
     np.testing.assert_array_equal(via_torch[quirk].view(np.uint32), ref[quirk].view(np.uint32))
+
+
+def test_modified_cosine_oracle_vs_matchms_restatement():
+    """The C restatement of matchms ModifiedCosine against the independent
+    pure-Python one (unshifted + precursor-shifted matches, one stable sort,
+    one greedy) on analogue families, where shifted matches matter."""
+    from cudams import synthetic
+
+    P, prec = synthetic.analog_spectra(24, seed=21, family_size=6)
+    s, m, o = oracle.modified_cosine(P, P, prec, prec, 0.05, 1 << 20)
+    assert not o.any()
+    plain, _, _ = oracle.cosine_greedy(P, P, 0.05, 0.0, 1 << 20)
+    assert (s > plain + 1e-3).sum() > 20  # the shifted matches raise many scores
+    for i in range(P.n):
+        r0, r1 = P.offsets[i:i + 2]
+        for j in range(P.n):
+            q0, q1 = P.offsets[j:j + 2]
+            rs, rm = matchms_restated.modified_cosine_pair(
+                P.mz[r0:r1], P.b[r0:r1], P.mz[q0:q1], P.b[q0:q1], prec[i], prec[j], 0.05)
+            assert m[i, j] == rm, (i, j)
+            assert abs(float(s[i, j]) - rs) <= 1e-6, (i, j)
+
+
+def test_modified_cosine_oracle_match_limit():
+    """Generation stops at match_limit over the concatenated (unshifted, then
+    shifted) order and sets overflow; the survivors are a prefix."""
+    from cudams import synthetic
+
+    P, prec = synthetic.analog_spectra(16, seed=22, family_size=4)
+    full = oracle.modified_cosine(P, P, prec, prec, 0.05, 1 << 20)
+    lim = oracle.modified_cosine(P, P, prec, prec, 0.05, 6)
+    assert lim[2].any() and not full[2].any()
+    ok = lim[2] == 0
+    np.testing.assert_array_equal(lim[1][ok], full[1][ok])
+    np.testing.assert_array_equal(lim[0][ok], full[0][ok])
+    assert (lim[1] <= 6).all()
