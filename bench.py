@@ -420,6 +420,12 @@ def run_ours(args, world, rank, local):
         plain_rate = prow * Q / (pms / 1000.0)
         line["plain"] = {"value": plain_rate, "unit": UNIT,
                          "sample": f"{prow} reference rows x {Q} queries, one launch"}
+        try:
+            line["plain"]["reference_numba_kernel"] = time_reference_kernel(
+                ref, qry, TOL, MATCH_LIMIT, N_MAX_PEAKS, 2048)
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            line["plain"]["reference_numba_kernel"] = {"unavailable":
+                                                       f"{type(e).__name__}: {e}"[:300]}
         line["speedup_vs_plain"] = value / world / plain_rate
 
     # end to end through the public API from host spectra
@@ -457,6 +463,103 @@ def run_ours(args, world, rank, local):
         line["served"] = served_workload(dev, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+REF_SSF = ROOT / "baseline" / "_ref" / "cudams" / "similarity" / "spectrum_similarity_functions.py"
+
+
+def reference_gpu_kernel():
+    """The reference's own Numba kernel factory (cosine_greedy_kernel,
+    spectrum_similarity_functions.py:12-278) from the unmodified install in
+    baseline/_ref, or (None, reason).  Its module imports matchms only for the
+    CPU helpers the kernel does not use; stand-ins fill those names."""
+    import importlib.util
+    import types
+
+    if not REF_SSF.exists():
+        return None, "reference not installed in baseline/_ref"
+    try:
+        from numba import cuda
+
+        if not cuda.is_available():
+            return None, "numba reports no CUDA device"
+        for name, attrs in (("matchms", {}), ("matchms.similarity", {}),
+                            ("matchms.similarity.spectrum_similarity_functions",
+                             {"collect_peak_pairs": None, "score_best_matches": None})):
+            if name not in sys.modules:
+                m = types.ModuleType(name)
+                m.__dict__.update(attrs)
+                sys.modules[name] = m
+        spec = importlib.util.spec_from_file_location("cudams_reference_ssf", REF_SSF)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        return mod.cosine_greedy_kernel, ""
+    except Exception as e:  # noqa: BLE001 - reported, not fatal
+        return None, f"{type(e).__name__}: {str(e)[:200]}"
+
+
+def time_reference_kernel(packed_r, packed_q, tol, match_limit, n_max_peaks, batch):
+    """pairs/s of the reference kernel on one batch x batch launch (its own
+    padded [2, B, n_max_peaks] layout, CudaCosineGreedy.py:63-87), inputs on
+    the device; or {"unavailable": reason}."""
+    import numpy as np
+    import torch
+
+    factory, why = reference_gpu_kernel()
+    if factory is None:
+        return {"unavailable": why}
+    from numba import cuda
+
+    def padded(p, n):
+        spec = np.zeros((2, batch, n_max_peaks), np.float32)
+        lens = np.zeros(batch, np.int32)
+        for i in range(min(n, p.n)):
+            a, b = p.offsets[i], min(p.offsets[i + 1], p.offsets[i] + n_max_peaks)
+            spec[0, i, :b - a] = p.mz[a:b]
+            spec[1, i, :b - a] = p.b[a:b]
+            lens[i] = b - a
+        return spec, lens
+
+    nr, nq = min(batch, packed_r.n), min(batch, packed_q.n)
+    rs, rl = padded(packed_r, nr)
+    qs, ql = padded(packed_q, nq)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rspec = torch.from_numpy(rs).to(dev)
+    qspec = torch.from_numpy(qs).to(dev)
+    lens = torch.from_numpy(np.stack([rl, ql])).to(dev)
+    out = torch.empty((3, batch, batch), dtype=torch.float32, device=dev)
+    kern = factory(tolerance=tol, shift=0.0, mz_power=0.0, int_power=1.0,
+                   match_limit=match_limit, batch_size=batch, n_max_peaks=n_max_peaks)
+    args = [cuda.as_cuda_array(t) for t in (rspec, qspec, lens, out)]
+    kern(*args)  # JIT compile + warm-up
+    cuda.synchronize()
+    t0 = time.perf_counter()
+    kern(*args)
+    cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"pairs_per_s": nr * nq / dt, "ms": 1e3 * dt, "batch": batch,
+            "sample": f"{nr} x {nq} pairs in one {batch} x {batch} launch",
+            "source": "baseline/_ref (unmodified reference), numba.cuda JIT for this GPU"}
+
+
+class _Peaks:
+    def __init__(self, mz, intensities):
+        self.mz, self.intensities = mz, intensities
+
+
+class _Spectrum:
+    """A matchms-like spectrum (peaks.mz / peaks.intensities, float64)."""
+
+    def __init__(self, mz, intensities):
+        self.peaks = _Peaks(mz, intensities)
+
+
+def _as_spectra(packed):
+    import numpy as np
+
+    off = packed.offsets
+    return [_Spectrum(packed.mz[off[i]:off[i + 1]].astype(np.float64),
+                      packed.b[off[i]:off[i + 1]].astype(np.float64)) for i in range(packed.n)]
 
 
 def _time_ms(fn, reps=3):
@@ -568,11 +671,37 @@ def other_workloads(dev, args):
     finally:
         gctx.graph_enable(False)
     ms_p = _time_ms(lambda: kernels.cosine_greedy_plain(u_r, u_q, 0.1, 0.0, 2048, 1024))
+    # end to end from matchms-like Spectrum objects, as the reference's
+    # published timings are taken: per-spectrum packing, H2D, kernels, D2H of
+    # the dense [3, 1024, 1024] result into a structured array
+    from cudams.similarity import CudaCosineGreedy
+
+    sr = _as_spectra(synthetic.uniform_spectra(1024, seed=args.seed + 1))
+    sq = _as_spectra(synthetic.uniform_spectra(1024, seed=args.seed + 2))
+    cg = CudaCosineGreedy(tolerance=0.1, match_limit=2048)
+    cg.matrix(sr, sq)
+    e2e_s = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        cg.matrix(sr, sq)
+        e2e_s.append(time.perf_counter() - t0)
+    try:
+        ref_k = time_reference_kernel(synthetic.uniform_spectra(1024, seed=args.seed + 1),
+                                      synthetic.uniform_spectra(1024, seed=args.seed + 2), 0.1,
+                                      2048, 1024, 1024)
+    except Exception as e:  # noqa: BLE001 - reported, not fatal
+        ref_k = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     res["uniform_1k"] = {"workload": "1024 x 1024, peaks U{10..200}, tol 0.1, match_limit 2048",
                          "tiled_pairs_per_s": 1024 * 1024 / (ms_t / 1e3),
                          "tiled_graph_pairs_per_s": 1024 * 1024 / (ms_g / 1e3),
-                         "plain_pairs_per_s": 1024 * 1024 / (ms_p / 1e3), "tiled_ms": ms_t,
-                         "tiled_graph_ms": ms_g, "tuning": u_cfg}
+                         "plain_pairs_per_s": 1024 * 1024 / (ms_p / 1e3),
+                         "reference_numba_kernel": ref_k, "tiled_ms": ms_t,
+                         "tiled_graph_ms": ms_g, "tuning": u_cfg,
+                         "e2e_from_spectrum_objects": {
+                             "pairs_per_s": 1024 * 1024 / statistics.median(e2e_s),
+                             "ms": 1e3 * statistics.median(e2e_s),
+                             "path": "CudaCosineGreedy.matrix(list of Spectrum objects) -> "
+                                     "numpy structured array (packing + H2D + kernels + D2H)"}}
 
     # overflow stress: clustered dense spectra, 20k x 20k, nearly every pair overflows
     c_r = synthetic.clustered_spectra(20_000, seed=args.seed + 3)
@@ -600,11 +729,80 @@ def other_workloads(dev, args):
     return res
 
 
-def served_workload(dev, args, seconds: float = 15.0, rate_1k: float = 20.0,
-                    rate_bg: float = 20.0, library_size: int = 1_000_000):
-    """Resident 1M-spectrum library, Poisson-arriving query batches: 1000-query
-    batches at rate_1k per second plus background batches of log-uniform size in
-    [1, 4096] at rate_bg per second; sparse output of scores >= 0.7."""
+def _offered_load(srv, pool, rng, rate_1k: float, rate_bg: float, seconds: float):
+    """Poisson arrivals for `seconds`: 1000-query batches at rate_1k/s plus
+    background batches of log-uniform size in [1, 4096] at rate_bg/s."""
+    import numpy as np
+
+    futs, kinds = [], []
+    t0 = time.perf_counter()
+    nxt1 = t0 + rng.exponential(1 / rate_1k)
+    nxt2 = t0 + (rng.exponential(1 / rate_bg) if rate_bg > 0 else float("inf"))
+    off = 0
+    while True:
+        now = time.perf_counter()
+        if now - t0 >= seconds:
+            break
+        if now >= nxt1:
+            futs.append(srv.submit(pool.subset(off % 59000, off % 59000 + 1000)))
+            kinds.append(1000)
+            off += 1000
+            nxt1 += rng.exponential(1 / rate_1k)
+        if now >= nxt2:
+            k = int(np.exp(rng.uniform(0.0, np.log(4096.0))))
+            futs.append(srv.submit(pool.subset(off % 55000, off % 55000 + k)))
+            kinds.append(k)
+            off += k
+            nxt2 += rng.exponential(1 / rate_bg)
+        time.sleep(max(0.0, min(nxt1, nxt2) - time.perf_counter() - 2e-4))
+    res = [f.result() for f in futs]
+    elapsed = time.perf_counter() - t0
+    lat_1k = np.array([r.latency_s for r, k in zip(res, kinds) if k == 1000]) * 1e3
+    lat = np.array([r.latency_s for r in res]) * 1e3
+    return {"offered_1k_per_s": rate_1k, "offered_background_per_s": rate_bg,
+            "seconds": seconds, "requests": len(res), "requests_1k": int(lat_1k.size),
+            "p50_ms_1k": float(np.percentile(lat_1k, 50)),
+            "p99_ms_1k": float(np.percentile(lat_1k, 99)),
+            "p99_ms_all": float(np.percentile(lat, 99)),
+            "pairs_per_s": sum(r.pairs for r in res) / elapsed,
+            "hits": int(sum(r.ref.shape[0] for r in res))}
+
+
+def _saturated(srv, pool, clients: int, seconds: float):
+    """Closed loop: `clients` threads each submit a 1000-query batch as soon as
+    their previous one returns, for `seconds`."""
+    import numpy as np
+
+    lats, pairs = [], [0]
+    lock = threading.Lock()
+    t_end = time.perf_counter() + seconds
+
+    def client(i):
+        off = 1000 * i
+        while time.perf_counter() < t_end:
+            r = srv.submit(pool.subset(off % 59000, off % 59000 + 1000)).result()
+            off += 1000 * clients
+            with lock:
+                lats.append(r.latency_s * 1e3)
+                pairs[0] += r.pairs
+
+    t0 = time.perf_counter()
+    ts = [threading.Thread(target=client, args=(i,)) for i in range(clients)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    elapsed = time.perf_counter() - t0
+    return {"clients": clients, "seconds": seconds, "requests": len(lats),
+            "pairs_per_s": pairs[0] / elapsed, "p50_ms_1k": float(np.percentile(lats, 50)),
+            "p99_ms_1k": float(np.percentile(lats, 99))}
+
+
+def served_workload(dev, args, library_size: int = 1_000_000):
+    """Resident 1M-spectrum library, sparse output of scores >= 0.7: latency of
+    one 1000-query batch alone; p50/p99 under two Poisson offered loads
+    (1000-query batches plus log-uniform [1, 4096]-query background batches);
+    saturated throughput from closed-loop clients."""
     import numpy as np
     import torch
 
@@ -621,47 +819,25 @@ def served_workload(dev, args, seconds: float = 15.0, rate_1k: float = 20.0,
     alone = []
     for i in range(5):
         alone.append(lib.search(pool.subset(1000 * i, 1000 * (i + 1)), 0.7).latency_s)
-    futs, kinds = [], []
     try:
         with Server(lib, threshold=0.7, slots=4) as srv:
-            t0 = time.perf_counter()
-            nxt1 = t0 + rng.exponential(1 / rate_1k)
-            nxt2 = t0 + rng.exponential(1 / rate_bg)
-            off = 0
-            while True:
-                now = time.perf_counter()
-                if now - t0 >= seconds:
-                    break
-                if now >= nxt1:
-                    futs.append(srv.submit(pool.subset(off % 59000, off % 59000 + 1000)))
-                    kinds.append(1000)
-                    off += 1000
-                    nxt1 += rng.exponential(1 / rate_1k)
-                if now >= nxt2:
-                    k = int(np.exp(rng.uniform(0.0, np.log(4096.0))))
-                    futs.append(srv.submit(pool.subset(off % 55000, off % 55000 + k)))
-                    kinds.append(k)
-                    off += k
-                    nxt2 += rng.exponential(1 / rate_bg)
-                time.sleep(max(0.0, min(nxt1, nxt2) - time.perf_counter() - 2e-4))
-            res = [f.result() for f in futs]
-            elapsed = time.perf_counter() - t0
+            loads = [_offered_load(srv, pool, rng, r1, 20.0, 10.0) for r1 in (20.0, 60.0)]
+            sat = _saturated(srv, pool, clients=8, seconds=8.0)
             concurrent = srv.max_concurrent
     finally:
         lib.close()
-    lat_1k = np.array([r.latency_s for r, k in zip(res, kinds) if k == 1000]) * 1e3
-    lat = np.array([r.latency_s for r in res]) * 1e3
+    base = loads[0]
     return {
         "workload": f"resident library of {library_size} lognormal spectra, tol {TOL}, "
-                    f"match_limit {MATCH_LIMIT}; Poisson arrivals: 1000-query batches at "
-                    f"{rate_1k}/s + log-uniform [1, 4096]-query batches at {rate_bg}/s for "
-                    f"{seconds:.0f} s; sparse output score >= 0.7; 4 slots",
-        "library_build_s": build_s, "requests": len(res), "requests_1k": int(lat_1k.size),
-        "p50_ms_1k": float(np.percentile(lat_1k, 50)), "p99_ms_1k": float(np.percentile(lat_1k, 99)),
-        "p50_ms_all": float(np.percentile(lat, 50)), "p99_ms_all": float(np.percentile(lat, 99)),
+                    f"match_limit {MATCH_LIMIT}; sparse output score >= 0.7; 4 slots; "
+                    "offered loads: Poisson 1000-query batches at 20/s or 60/s plus "
+                    "log-uniform [1, 4096]-query batches at 20/s, 10 s each; saturated: 8 "
+                    "closed-loop clients of 1000-query batches, 8 s",
+        "library_build_s": build_s,
         "latency_1k_alone_ms": float(1e3 * np.median(alone)),
-        "pairs_per_s": sum(r.pairs for r in res) / elapsed,
-        "max_concurrent_requests": concurrent, "hits": int(sum(r.ref.shape[0] for r in res))}
+        "p50_ms_1k": base["p50_ms_1k"], "p99_ms_1k": base["p99_ms_1k"],
+        "offered_loads": loads, "saturated": sat,
+        "pairs_per_s": base["pairs_per_s"], "max_concurrent_requests": concurrent}
 
 
 def main():
