@@ -28,6 +28,7 @@ struct SpecSet {
     const int64_t* off;
     int64_t n;
     int64_t n_peaks;
+    const double* prec = nullptr;  // precursor m/z per spectrum (modified cosine only)
 };
 
 struct CosineArgs {
@@ -36,6 +37,9 @@ struct CosineArgs {
     double tol;
     double shift;
     int match_limit;
+    // modified cosine: candidates at shift 0 followed by those at the
+    // precursor difference prec_ref - prec_query (ref.prec / qry.prec set)
+    bool modified = false;
 };
 
 struct DenseOut {

@@ -63,20 +63,22 @@ constexpr int kLongRun = 32;      // longer runs go to the pair kernel
 constexpr int kMidRun = 8;        // runs up to this length are resolved four per warp step
 constexpr int kMaxTile = 4096;    // max query spectra per tile
 constexpr int kOrderClasses = 17; // log2 length classes (0..16)
+constexpr int kModifiedMaxPeaks = 32767;  // modified cosine: reference peak index in 15 bits
 
 __device__ __forceinline__ double peak_a(const double* a, int64_t i) { return a ? a[i] : 1.0; }
 
 // ---------------------------------------------------------------------------
 // 1. validation
 // ---------------------------------------------------------------------------
-__global__ void validate_kernel(SpecSet S, uint32_t* bad, uint32_t* err) {
+__global__ void validate_kernel(SpecSet S, uint32_t* bad, uint32_t* err,
+                                int max_peaks = CMS_MAX_PEAKS) {
     const int64_t n = S.n;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n;
          s += (int64_t)gridDim.x * blockDim.x) {
         const int64_t lo = S.off[s], hi = S.off[s + 1];
         uint32_t e = 0;
         if (lo < 0 || hi < lo || hi > S.n_peaks) e |= kErrBadOffsets;
-        if (hi - lo > CMS_MAX_PEAKS) e |= kErrSpectrumTooLong;
+        if (hi - lo > max_peaks) e |= kErrSpectrumTooLong;
         if (e) {
             atomicOr(err, e);
             atomicOr(bad, 1u);
@@ -160,7 +162,18 @@ __device__ __forceinline__ long long bucket_of(float x, double inv_w) {
     return __double2ll_rd(__dmul_rn((double)x, inv_w));
 }
 
+// The value an index sorts a peak by: its m/z, or for the neutral-loss index
+// of modified cosine (NL) its m/z minus its spectrum's precursor m/z, computed
+// in float64 and rounded to float32 (the join widens its windows by a margin
+// that covers this rounding and confirms each candidate exactly).
+template <bool NL>
+__device__ __forceinline__ float index_value(const SpecSet& B, int64_t s, int64_t k) {
+    if (!NL) return B.mz[k];
+    return __double2float_rn(__dsub_rn((double)B.mz[k], B.prec[s]));
+}
+
 // warp per spectrum: histogram of (tile, bucket)
+template <bool NL>
 __global__ void index_count_kernel(SpecSet B, IndexGeom g, uint32_t* cnt, const uint32_t* bad) {
     if (*bad) return;
     const int lane = threadIdx.x & 31;
@@ -172,7 +185,7 @@ __global__ void index_count_kernel(SpecSet B, IndexGeom g, uint32_t* cnt, const 
         const int64_t lo = B.off[s], hi = B.off[s + 1];
         uint32_t* c = cnt + t * (int64_t)g.nb;
         for (int64_t k = lo + lane; k < hi; k += 32) {
-            const unsigned bk = (unsigned)bucket_of(B.mz[k], g.inv_w) & mask;
+            const unsigned bk = (unsigned)bucket_of(index_value<NL>(B, s, k), g.inv_w) & mask;
             atomicAdd(&c[bk], 1u);
         }
     }
@@ -223,7 +236,8 @@ __global__ void index_scan_kernel(IndexGeom g, uint32_t* cnt_cur, uint32_t* tab,
     if (threadIdx.x == blockDim.x - 1) out[g.nb] = run;
 }
 
-// warp per spectrum: scatter (m/z, q_local<<16 | peak) into the tile stream
+// warp per spectrum: scatter (value, q_local<<16 | peak) into the tile stream
+template <bool NL>
 __global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, Entry* ent,
                                      const uint32_t* bad) {
     if (*bad) return;
@@ -238,7 +252,7 @@ __global__ void index_scatter_kernel(SpecSet B, IndexGeom g, uint32_t* cur, Entr
         const int64_t lo = B.off[s], hi = B.off[s + 1];
         uint32_t* c = cur + t * (int64_t)g.nb;
         for (int64_t k = lo + lane; k < hi; k += 32) {
-            const float mz = B.mz[k];
+            const float mz = index_value<NL>(B, s, k);
             const unsigned bk = (unsigned)bucket_of(mz, g.inv_w) & mask;
             const uint32_t pos = atomicAdd(&c[bk], 1u);
             Entry en;
@@ -326,6 +340,8 @@ struct JoinParams {
     const int32_t* a_order;
     const uint32_t* tab;
     const Entry* ent;
+    const uint32_t* tab2;  // modified cosine: neutral-loss index (m/z - precursor)
+    const Entry* ent2;
     IndexGeom g;
     double tol;
     double shift;
@@ -405,10 +421,35 @@ struct Pool {
 //   runs  uint32 [kLongRuns] runs of 4..32 candidates queued for the warp:
 //                            slot of the chain head | length << 12; runs of at
 //                            most kMidRun from the front, longer ones from the back
+//   x     float  [32]        per-lane sweeping-peak m/z (modified cosine's exact test)
 constexpr int kLongRuns = 64;
 __host__ __device__ constexpr int head_words(int tile) { return (((tile + 1) / 2) + 3) & ~3; }
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
-    return 16 * kPool + 4 * head_words(tile) + 8 * 32 + 8 * 32 + 4 * kLongRuns;
+    return 16 * kPool + 4 * head_words(tile) + 8 * 32 + 8 * 32 + 4 * kLongRuns + 4 * 32;
+}
+
+// Reference peak of a candidate's generation word.  Modified cosine marks
+// candidates of its second (precursor-shifted) pass in bit 31, which makes
+// them later in generation order than every unshifted one (the order of
+// matchms' concatenation) and limits its spectra to 32767 peaks.
+template <bool MODIFIED>
+__device__ __forceinline__ uint32_t gen_p1(uint32_t g) {
+    return MODIFIED ? ((g >> 16) & 0x7FFFu) : (g >> 16);
+}
+
+// Neutral-loss window of modified cosine's shifted pass: entries whose
+// m/z - precursor lies within tol of the sweeping peak's, widened by twice
+// the float32 spacing there (the stored values are rounded to float32) and a
+// float64 rounding allowance, rounded outwards; every entry inside is then
+// confirmed with the exact test of the shifted window.
+__device__ __forceinline__ bool nl_window(float mz, double prec, double tol, float& L, float& H) {
+    const double zr = __dsub_rn((double)mz, prec);
+    const float mag = __double2float_ru(fabs(zr) + tol + 1.0);
+    const double m = 2.0 * (double)(nextafterf(mag, INFINITY) - mag) +
+                     1e-9 * (fabs((double)mz) + fabs(prec) + 1.0);
+    L = __double2float_rd(__dsub_rn(__dsub_rn(zr, tol), m));
+    H = __double2float_ru(__dadd_rn(__dadd_rn(zr, tol), m));
+    return isfinite(L) && isfinite(H);
 }
 
 // Exact float32 window of one sweeping peak.
@@ -474,7 +515,7 @@ struct Window {
 };
 
 // Three CTAs (24 warps) per SM: up to 85 registers a thread.
-template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
+template <bool A_IS_REF, bool SPARSE, bool NOSHIFT, bool MODIFIED>
 __global__ void __launch_bounds__(kJoinThreads, 3)
 join_kernel(JoinParams P) {
     if (*P.bad) return;
@@ -485,6 +526,7 @@ join_kernel(JoinParams P) {
     double* s_wa = reinterpret_cast<double*>(slice + 16 * kPool + 4 * hw);
     float2* s_lh = reinterpret_cast<float2*>(slice + 16 * kPool + 4 * hw + 8 * 32);
     uint32_t* long_runs = reinterpret_cast<uint32_t*>(slice + 16 * kPool + 4 * hw + 16 * 32);
+    float* s_x = reinterpret_cast<float*>(slice + 16 * kPool + 4 * hw + 16 * 32 + 4 * kLongRuns);
     Pool pool;
     {
         const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
@@ -531,6 +573,7 @@ join_kernel(JoinParams P) {
         const int tn = (int)min((int64_t)P.g.tile, P.B.n - b_begin);
         const int64_t tbase = P.B.off[b_begin];
         const uint32_t* T = tab + (int64_t)t * (P.g.nb + 1);
+        const uint32_t* T2 = MODIFIED ? P.tab2 + (int64_t)t * (P.g.nb + 1) : nullptr;
         const double snA = P.snA[a];
         // a resolved run's result, stored straight into the dense output
         auto put_dense = [&](int bq, float sc, int mt) {
@@ -596,10 +639,22 @@ join_kernel(JoinParams P) {
                     nx_mz = P.A.mz[a0 + p + 32];
                     nx_w = __dmul_rn(peak_a(P.A.a, a0 + p + 32), P.A.b[a0 + p + 32]);
                 }
+                s_wa[lane] = wA;
+                if (MODIFIED) s_x[lane] = mzA;
+                // modified cosine sweeps the chunk twice: at shift 0 through
+                // the m/z index, then at each query's precursor difference
+                // through the neutral-loss index
+#pragma unroll 1
+                for (int pass = 0; pass < (MODIFIED ? 2 : 1); ++pass) {
+                const uint32_t* TT = (MODIFIED && pass) ? T2 : T;
+                const Entry* EE = (MODIFIED && pass) ? P.ent2 : ent;
                 float L = 1.0f, H = 0.0f;
                 uint32_t r0b = 0, c0 = 0, r1b = 0, c1 = 0;
                 if (p < na) {
-                    if (!Window<A_IS_REF, NOSHIFT>::bounds(mzA, P.tol, P.shift, L, H)) {
+                    const bool ok = (MODIFIED && pass)
+                                        ? nl_window(mzA, P.A.prec[a], P.tol, L, H)
+                                        : Window<A_IS_REF, NOSHIFT>::bounds(mzA, P.tol, P.shift, L, H);
+                    if (!ok) {
                         atomicOr(P.err, kErrBadOffsets);
                         L = 1.0f;
                         H = 0.0f;
@@ -608,22 +663,21 @@ join_kernel(JoinParams P) {
                         const long long blo = bucket_of(L, P.g.inv_w);
                         const long long bhi = bucket_of(H, P.g.inv_w);
                         if (bhi - blo + 1 >= P.g.nb) {
-                            r0b = __ldg(&T[0]);
-                            c0 = __ldg(&T[P.g.nb]) - r0b;
+                            r0b = __ldg(&TT[0]);
+                            c0 = __ldg(&TT[P.g.nb]) - r0b;
                         } else {
                             const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
-                            r0b = __ldg(&T[bl]);
+                            r0b = __ldg(&TT[bl]);
                             if (bl <= bh) {
-                                c0 = __ldg(&T[bh + 1]) - r0b;
+                                c0 = __ldg(&TT[bh + 1]) - r0b;
                             } else {
-                                c0 = __ldg(&T[P.g.nb]) - r0b;
-                                r1b = __ldg(&T[0]);
-                                c1 = __ldg(&T[bh + 1]) - r1b;
+                                c0 = __ldg(&TT[P.g.nb]) - r0b;
+                                r1b = __ldg(&TT[0]);
+                                c1 = __ldg(&TT[bh + 1]) - r1b;
                             }
                         }
                     }
                 }
-                s_wa[lane] = wA;
                 s_lh[lane] = make_float2(L, H);
                 const uint32_t c = c0 + c1;
                 uint32_t incl = c;
@@ -660,10 +714,20 @@ join_kernel(JoinParams P) {
                     Entry en;
                     en.id = 0;
                     if (k < E) {
-                        en = ent[tbase + pos];
+                        en = EE[tbase + pos];
                         const float2 lh = s_lh[o];
                         const int bq = (int)(en.id >> 16);
                         cand = en.mz >= lh.x && en.mz <= lh.y && bq >= range_lo && bq < range_hi;
+                        if (MODIFIED && pass && cand) {
+                            // the shifted window exactly as matchms tests it:
+                            // mz2 = mz_q + (prec_ref - prec_q) against mz_ref -+ tol
+                            const int qb = b_begin + bq;
+                            const float y = P.B.mz[P.B.off[qb] + (en.id & 0xFFFFu)];
+                            const double mz2 =
+                                __dadd_rn((double)y, __dsub_rn(P.A.prec[a], P.B.prec[qb]));
+                            const double x = (double)s_x[o];
+                            cand = !(mz2 > __dadd_rn(x, P.tol)) && !(mz2 < __dsub_rn(x, P.tol));
+                        }
                     }
                     const unsigned bal = __ballot_sync(full, cand);
                     const int slot = n + __popc(bal & below);
@@ -678,6 +742,7 @@ join_kernel(JoinParams P) {
                         if (A_IS_REF) {
                             key = __dmul_rn(__dmul_rn(s_wa[o], aB), en.b);
                             gen = ((uint32_t)pa << 16) | (uint32_t)pB;
+                            if (MODIFIED) gen |= (uint32_t)pass << 31;
                         } else {
                             const double wB = __dmul_rn(aB, en.b);
                             key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + pa)), P.A.b[a0 + pa]);
@@ -702,7 +767,9 @@ join_kernel(JoinParams P) {
                     }
                     if (n > P.pool_max) break;
                 }
-                __syncwarp();  // s_wa / s_lh are rewritten by the next chunk
+                __syncwarp();  // s_lh / s_wa / s_x are rewritten by the next pass or chunk
+                if (n > P.pool_max) break;
+                }
                 if (n > P.pool_max) break;
             }
             __syncwarp();
@@ -814,7 +881,7 @@ join_kernel(JoinParams P) {
                         if (mine) {
                             score = __dadd_rn(score, lk);
                             ++mt;
-                            if (lane == leader || ((g >> 16) == (lg >> 16)) ||
+                            if (lane == leader || gen_p1<MODIFIED>(g) == gen_p1<MODIFIED>(lg) ||
                                 ((g & 0xFFFFu) == (lg & 0xFFFFu)))
                                 alive = false;
                         }
@@ -863,8 +930,8 @@ join_kernel(JoinParams P) {
                         const double lk = __shfl_sync(full, k, leader);
                         score = __dadd_rn(score, lk);
                         ++mt;
-                        if (lane == leader ||
-                            ((g >> 16) == (lg >> 16)) || ((g & 0xFFFFu) == (lg & 0xFFFFu)))
+                        if (lane == leader || gen_p1<MODIFIED>(g) == gen_p1<MODIFIED>(lg) ||
+                            ((g & 0xFFFFu) == (lg & 0xFFFFu)))
                             alive = false;
                         bal = __ballot_sync(full, alive);
                     }
@@ -944,7 +1011,8 @@ join_kernel(JoinParams P) {
                                 }
                             };
                             auto clash = [](uint32_t ga, uint32_t gb) {
-                                return (ga >> 16) == (gb >> 16) || (ga & 0xFFFFu) == (gb & 0xFFFFu);
+                                return gen_p1<MODIFIED>(ga) == gen_p1<MODIFIED>(gb) ||
+                                       (ga & 0xFFFFu) == (gb & 0xFFFFu);
                             };
                             order(k0, g0, k1, g1);
                             if (L == 3) {
@@ -1105,7 +1173,7 @@ __device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m) {
     __syncthreads();
 }
 
-template <bool SPARSE>
+template <bool SPARSE, bool MODIFIED>
 __global__ void pair_kernel(PairParams P) {
     if (*P.bad) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1146,7 +1214,12 @@ __global__ void pair_kernel(PairParams P) {
 
         int total = 0;
         bool overflow = false;
-        if (nr > 0 && nq > 0) {
+        // modified cosine generates twice: at shift 0, then at the pair's
+        // precursor difference, continuing the same candidate list
+#pragma unroll 1
+        for (int pass = 0; pass < (MODIFIED ? 2 : 1) && !overflow && nr > 0 && nq > 0; ++pass) {
+            const double shift =
+                (MODIFIED && pass) ? __dsub_rn(P.R.prec[ri], P.Q.prec[qi]) : P.shift;
             for (int pc = 0; pc < nr && !overflow; pc += blockDim.x) {
                 const int p1 = pc + tid;
                 int start = 0, cnt = 0;
@@ -1159,14 +1232,14 @@ __global__ void pair_kernel(PairParams P) {
                     int L = 0, H = nq;
                     while (L < H) {
                         const int M = (L + H) >> 1;
-                        if (__dadd_rn((double)qmz[M], P.shift) < lo)
+                        if (__dadd_rn((double)qmz[M], shift) < lo)
                             L = M + 1;
                         else
                             H = M;
                     }
                     start = L;
                     int k = L;
-                    while (k < nq && !(__dadd_rn((double)qmz[k], P.shift) > hi)) ++k;
+                    while (k < nq && !(__dadd_rn((double)qmz[k], shift) > hi)) ++k;
                     cnt = k - L;
                 }
                 // block exclusive scan of cnt
@@ -1199,7 +1272,7 @@ __global__ void pair_kernel(PairParams P) {
                         const double key =
                             __dmul_rn(__dmul_rn(w1, peak_a(P.Q.a, q0 + p2)), P.Q.b[q0 + p2]);
                         okey[rank] = order_key(key);
-                        cgen[rank] = ((uint32_t)p1 << 16) | (uint32_t)p2;
+                        cgen[rank] = ((uint32_t)pass << 31) | ((uint32_t)p1 << 16) | (uint32_t)p2;
                     }
                 }
                 total += chunk_total;
@@ -1268,7 +1341,7 @@ __global__ void pair_kernel(PairParams P) {
                     }
                     bool alive = false;
                     if (i < n) {
-                        const int p1 = g >> 16, p2 = g & 0xFFFF;
+                        const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
                         alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
                                 !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
                     }
@@ -1276,7 +1349,8 @@ __global__ void pair_kernel(PairParams P) {
                     if (live == 0u) continue;
                     // dead lanes get values no peak index takes, so they match
                     // only themselves
-                    const unsigned m1 = __match_any_sync(full, alive ? (g >> 16) : 0x10000u + lane);
+                    const unsigned m1 =
+                        __match_any_sync(full, alive ? gen_p1<MODIFIED>(g) : 0x10000u + lane);
                     const unsigned m2 =
                         __match_any_sync(full, alive ? (g & 0xFFFFu) : 0x10000u + lane);
                     const unsigned earlier = (m1 | m2) & live & below;
@@ -1291,7 +1365,7 @@ __global__ void pair_kernel(PairParams P) {
                         acc = __ballot_sync(full, my_acc);
                     }
                     if ((acc >> lane) & 1u) {
-                        const int p1 = g >> 16, p2 = g & 0xFFFF;
+                        const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
                         atomicOr(&used_r[p1 >> 5], 1u << (p1 & 31));
                         atomicOr(&used_q[p2 >> 5], 1u << (p2 & 31));
                     }
@@ -1418,10 +1492,10 @@ int set_func_smem(T* f, size_t bytes) {
 // (jp.max_fetch > 0, no global pool): enough short-lived CTAs for the work,
 // each warp exiting after max_fetch fetches, so that the SMs free up CTA by
 // CTA and concurrent launches on other streams are scheduled in between.
-template <bool A_IS_REF, bool SPARSE, bool NOSHIFT>
+template <bool A_IS_REF, bool SPARSE, bool NOSHIFT, bool MODIFIED>
 int launch_join(cms_ctx* ctx, JoinParams jp, size_t smem, size_t gpool_warps, int64_t n_items,
                 cudaStream_t s) {
-    auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT>;
+    auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT, MODIFIED>;
     if (const int rc = set_func_smem(kern, smem)) return rc;
     jp.trace = TraceOut{ctx->trace_rec, ctx->trace_count, ctx->trace_cap, ctx->trace_tag};
     int64_t grid;
@@ -1485,6 +1559,11 @@ int run_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         need += bump_size((size_t)p.n_tiles * (p.nb + 1) * sizeof(uint32_t));
         need += bump_size((size_t)p.n_tiles * p.nb * sizeof(uint32_t));
         need += bump_size((size_t)std::max<int64_t>(1, args.qry.n_peaks) * sizeof(Entry));
+        if (args.modified) {  // the neutral-loss index
+            need += bump_size((size_t)p.n_tiles * (p.nb + 1) * sizeof(uint32_t));
+            need += bump_size((size_t)p.n_tiles * p.nb * sizeof(uint32_t));
+            need += bump_size((size_t)std::max<int64_t>(1, args.qry.n_peaks) * sizeof(Entry));
+        }
         need += bump_size((size_t)p.spill_cap * sizeof(int2));
         need += bump_size(gpool_bytes);
     }
@@ -1524,8 +1603,11 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     };
     {
         StageScope sc(ctx, 0, 4, s);
-        validate_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, bad, ctx->err_word);
-        validate_kernel<<<grid_for(nQ, threads), threads, 0, s>>>(args.qry, bad, ctx->err_word);
+        const int max_peaks = args.modified ? kModifiedMaxPeaks : CMS_MAX_PEAKS;
+        validate_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, bad, ctx->err_word,
+                                                                 max_peaks);
+        validate_kernel<<<grid_for(nQ, threads), threads, 0, s>>>(args.qry, bad, ctx->err_word,
+                                                                 max_peaks);
         norms_kernel<<<grid_for(nR, threads), threads, 0, s>>>(args.ref, snR, bad);
         norms_kernel<<<grid_for(nQ, threads), threads, 0, s>>>(args.qry, snQ, bad);
     }
@@ -1559,25 +1641,19 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         return launch_mirror(pp.dense, nR, bad, ctx->sm_count, s);
     };
 
+    void (*pair_k)(PairParams) =
+        sparse ? (args.modified ? pair_kernel<true, true> : pair_kernel<true, false>)
+               : (args.modified ? pair_kernel<false, true> : pair_kernel<false, false>);
     int pair_blocks_per_sm = 1;
-    if (sparse) {
-        if ((rc = set_func_smem(pair_kernel<true>, pair_smem))) return rc;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<true>,
-                                                      p.pair_threads, pair_smem);
-    } else {
-        if ((rc = set_func_smem(pair_kernel<false>, pair_smem))) return rc;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_kernel<false>,
-                                                      p.pair_threads, pair_smem);
-    }
+    if ((rc = set_func_smem(pair_k, pair_smem))) return rc;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_blocks_per_sm, pair_k, p.pair_threads,
+                                                  pair_smem);
     pair_blocks_per_sm = std::max(1, pair_blocks_per_sm);
     const int pair_grid = ctx->sm_count * pair_blocks_per_sm;
 
     if (p.mode == 2) {
         StageScope sc(ctx, 4, 1, s);
-        if (sparse)
-            pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
-        else
-            pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        pair_k<<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
         CMS_CUDA_TRY(cudaGetLastError());
         return mirror();
     }
@@ -1587,6 +1663,14 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     uint32_t* tab = bp.take<uint32_t>((size_t)p.n_tiles * (p.nb + 1));
     uint32_t* cur = bp.take<uint32_t>((size_t)p.n_tiles * p.nb);
     Entry* ent = bp.take<Entry>((size_t)std::max<int64_t>(1, args.qry.n_peaks));
+    uint32_t* tab2 = nullptr;
+    uint32_t* cur2 = nullptr;
+    Entry* ent2 = nullptr;
+    if (args.modified) {
+        tab2 = bp.take<uint32_t>((size_t)p.n_tiles * (p.nb + 1));
+        cur2 = bp.take<uint32_t>((size_t)p.n_tiles * p.nb);
+        ent2 = bp.take<Entry>((size_t)std::max<int64_t>(1, args.qry.n_peaks));
+    }
     int2* spill = bp.take<int2>(p.spill_cap);
     unsigned char* gpool = bp.take<unsigned char>(gpool_bytes);
 
@@ -1600,10 +1684,19 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     {
         StageScope sc(ctx, 2, 3, s);
         CMS_CUDA_TRY(cudaMemsetAsync(cur, 0, (size_t)p.n_tiles * p.nb * sizeof(uint32_t), s));
-        index_count_kernel<<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur, bad);
+        index_count_kernel<false><<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur, bad);
         index_scan_kernel<<<p.n_tiles, 1024, 0, s>>>(g, cur, tab, bad);
-        index_scatter_kernel<<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur,
+        index_scatter_kernel<false><<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur,
                                                                             ent, bad);
+    }
+    if (args.modified) {  // neutral-loss index: m/z - precursor, same geometry
+        StageScope sc(ctx, 2, 3, s);
+        CMS_CUDA_TRY(cudaMemsetAsync(cur2, 0, (size_t)p.n_tiles * p.nb * sizeof(uint32_t), s));
+        index_count_kernel<true><<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur2,
+                                                                                bad);
+        index_scan_kernel<<<p.n_tiles, 1024, 0, s>>>(g, cur2, tab2, bad);
+        index_scatter_kernel<true><<<grid_for(nQ * 32, threads), threads, 0, s>>>(args.qry, g, cur2,
+                                                                                  ent2, bad);
     }
     CMS_CUDA_TRY(cudaGetLastError());
 
@@ -1615,6 +1708,8 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     jp.a_order = order;
     jp.tab = tab;
     jp.ent = ent;
+    jp.tab2 = tab2;
+    jp.ent2 = ent2;
     jp.g = g;
     jp.tol = args.tol;
     jp.shift = args.shift;
@@ -1643,12 +1738,20 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
         StageScope sc(ctx, 3, 1, s);
         const bool noshift = args.shift == 0.0;
         const int64_t items = nR * (int64_t)p.n_tiles;
+        if (args.modified)  // shift 0 at the first pass; the second takes it per pair
+            rc = sparse ? launch_join<true, true, true, true>(ctx, jp, join_smem, gpool_warps, items, s)
+                        : launch_join<true, false, true, true>(ctx, jp, join_smem, gpool_warps, items,
+                                                                s);
+        else
         rc = sparse
-                 ? (noshift ? launch_join<true, true, true>(ctx, jp, join_smem, gpool_warps, items, s)
-                            : launch_join<true, true, false>(ctx, jp, join_smem, gpool_warps, items, s))
-                 : (noshift ? launch_join<true, false, true>(ctx, jp, join_smem, gpool_warps, items, s)
-                            : launch_join<true, false, false>(ctx, jp, join_smem, gpool_warps, items,
-                                                              s));
+                 ? (noshift ? launch_join<true, true, true, false>(ctx, jp, join_smem, gpool_warps,
+                                                                   items, s)
+                            : launch_join<true, true, false, false>(ctx, jp, join_smem, gpool_warps,
+                                                                    items, s))
+                 : (noshift ? launch_join<true, false, true, false>(ctx, jp, join_smem, gpool_warps,
+                                                                    items, s)
+                            : launch_join<true, false, false, false>(ctx, jp, join_smem, gpool_warps,
+                                                                     items, s));
         if (rc) return rc;
     }
     CMS_CUDA_TRY(cudaGetLastError());
@@ -1658,10 +1761,7 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     pp.pairs_cap = p.spill_cap;
     {
         StageScope sc(ctx, 4, 1, s);
-        if (sparse)
-            pair_kernel<true><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
-        else
-            pair_kernel<false><<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
+        pair_k<<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
         CMS_CUDA_TRY(cudaGetLastError());
     }
     return mirror();
@@ -1699,6 +1799,9 @@ int run_cosine_graph(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense
     put(args.tol);
     put(args.shift);
     put(args.match_limit);
+    put((int)args.modified);
+    put((uintptr_t)args.ref.prec);
+    put((uintptr_t)args.qry.prec);
     put((int)(dense != nullptr));
     if (dense) {
         put((uintptr_t)dense->score);
@@ -1859,6 +1962,78 @@ extern "C" int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const
     return run_cosine(ctx, args, nullptr, &out, cfg, s);
 }
 
+extern "C" int cms_modified_cosine(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                                   const double* ref_b, const int64_t* ref_off,
+                                   const double* ref_precursor, int64_t n_ref, int64_t n_ref_peaks,
+                                   const float* q_mz, const double* q_a, const double* q_b,
+                                   const int64_t* q_off, const double* q_precursor, int64_t n_q,
+                                   int64_t n_q_peaks, double tolerance, int match_limit,
+                                   float* score, int32_t* matches, uint8_t* overflow, int64_t ld,
+                                   const cms_cosine_config* cfg, void* stream) {
+    using namespace cms;
+    if (!ctx) {
+        set_error("cms_modified_cosine: null context");
+        return CMS_ERR_INVALID;
+    }
+    CosineArgs args{SpecSet{ref_mz, ref_a, ref_b, ref_off, n_ref, n_ref_peaks, ref_precursor},
+                    SpecSet{q_mz, q_a, q_b, q_off, n_q, n_q_peaks, q_precursor}, tolerance, 0.0,
+                    match_limit, true};
+    if (!check_common(args, "cms_modified_cosine")) return CMS_ERR_INVALID;
+    if (ld < n_q) {
+        set_error("cms_modified_cosine: ld < n_q");
+        return CMS_ERR_INVALID;
+    }
+    if (n_ref == 0 || n_q == 0) return CMS_OK;
+    if (!score || !matches || !overflow || !ref_precursor || !q_precursor) {
+        set_error("cms_modified_cosine: null output or precursor pointer");
+        return CMS_ERR_INVALID;
+    }
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    DenseOut out{score, matches, overflow, ld};
+    return run_cosine(ctx, args, &out, nullptr, cfg, (cudaStream_t)stream);
+}
+
+extern "C" int cms_modified_cosine_sparse(
+    cms_ctx* ctx, const float* ref_mz, const double* ref_a, const double* ref_b,
+    const int64_t* ref_off, const double* ref_precursor, int64_t n_ref, int64_t n_ref_peaks,
+    const float* q_mz, const double* q_a, const double* q_b, const int64_t* q_off,
+    const double* q_precursor, int64_t n_q, int64_t n_q_peaks, double tolerance, int match_limit,
+    float threshold, int32_t* hit_ref, int32_t* hit_query, float* hit_score, int32_t* hit_matches,
+    uint8_t* hit_overflow, int64_t capacity, int64_t* hit_count, const cms_cosine_config* cfg,
+    void* stream) {
+    using namespace cms;
+    if (!ctx) {
+        set_error("cms_modified_cosine_sparse: null context");
+        return CMS_ERR_INVALID;
+    }
+    CosineArgs args{SpecSet{ref_mz, ref_a, ref_b, ref_off, n_ref, n_ref_peaks, ref_precursor},
+                    SpecSet{q_mz, q_a, q_b, q_off, n_q, n_q_peaks, q_precursor}, tolerance, 0.0,
+                    match_limit, true};
+    if (!check_common(args, "cms_modified_cosine_sparse")) return CMS_ERR_INVALID;
+    if (!(threshold > 0.0f)) {
+        set_error("cms_modified_cosine_sparse: threshold must be > 0 (every pair scores >= 0)");
+        return CMS_ERR_INVALID;
+    }
+    if (capacity < 0 || !hit_count || (capacity > 0 && (!hit_ref || !hit_query || !hit_score ||
+                                                        !hit_matches || !hit_overflow))) {
+        set_error("cms_modified_cosine_sparse: invalid hit buffers");
+        return CMS_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    CMS_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (n_ref == 0 || n_q == 0) {
+        CMS_CUDA_TRY(cudaMemsetAsync(hit_count, 0, sizeof(int64_t), s));
+        return CMS_OK;
+    }
+    if (!ref_precursor || !q_precursor) {
+        set_error("cms_modified_cosine_sparse: null precursor pointer");
+        return CMS_ERR_INVALID;
+    }
+    SparseOut out{hit_ref, hit_query, hit_score, hit_matches, hit_overflow, capacity,
+                  reinterpret_cast<unsigned long long*>(hit_count), threshold};
+    return run_cosine(ctx, args, nullptr, &out, cfg, s);
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free variant (cms_cosine_greedy_noalloc)
 //
@@ -2013,11 +2188,11 @@ extern "C" int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_
     pp.bad = bad;
     const int pair_threads = 128;
     const size_t pair_smem = (size_t)cap * 12 + 2 * 2048 * 4;
-    if ((rc = set_func_smem(pair_kernel<false>, pair_smem))) return rc;
+    if ((rc = set_func_smem(pair_kernel<false, false>, pair_smem))) return rc;
     int per_sm = 1;
-    CMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<false>,
+    CMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<false, false>,
                                                                pair_threads, pair_smem));
-    pair_kernel<false><<<sms * std::max(1, per_sm), pair_threads, pair_smem, s>>>(pp);
+    pair_kernel<false, false><<<sms * std::max(1, per_sm), pair_threads, pair_smem, s>>>(pp);
     CMS_CUDA_TRY(cudaGetLastError());
     if (device_error)
         CMS_CUDA_TRY(cudaMemcpyAsync(device_error, err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -2117,9 +2292,9 @@ extern "C" int cms_library_create(cms_ctx* ctx, const float* mz, const double* a
     if (e == cudaSuccess) {
         validate_kernel<<<grid_for(n), threads, 0, s>>>(L->spec, L->bad, ctx->err_word);
         norms_kernel<<<grid_for(n), threads, 0, s>>>(L->spec, L->sn, L->bad);
-        index_count_kernel<<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->bad);
+        index_count_kernel<false><<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->bad);
         index_scan_kernel<<<L->g.n_tiles, 1024, 0, s>>>(L->g, cur, L->tab, L->bad);
-        index_scatter_kernel<<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->ent,
+        index_scatter_kernel<false><<<grid_for(n * 32), threads, 0, s>>>(L->spec, L->g, cur, L->ent,
                                                                   L->bad);
         e = cudaGetLastError();
     }
@@ -2260,8 +2435,9 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     jp.bad = bad;
     {
         StageScope sc(ctx, 3, 1, s);
-        rc = launch_join<false, true, false>(ctx, jp, (size_t)jp.warp_smem_bytes * kJoinWarps, 0,
-                                             items, s);
+        rc = launch_join<false, true, false, false>(ctx, jp,
+                                                    (size_t)jp.warp_smem_bytes * kJoinWarps, 0,
+                                                    items, s);
         if (rc) return rc;
     }
     PairParams pp{};
@@ -2283,10 +2459,11 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     pp.bad = bad;
     {
         StageScope sc(ctx, 4, 1, s);
-        if ((rc = set_func_smem(pair_kernel<true>, pair_smem))) return rc;
+        if ((rc = set_func_smem(pair_kernel<true, false>, pair_smem))) return rc;
         int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<true>, 128, pair_smem);
-        pair_kernel<true><<<std::max(1, std::min(ctx->sm_count * std::max(1, per_sm),
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel<true, false>, 128,
+                                                      pair_smem);
+        pair_kernel<true, false><<<std::max(1, std::min(ctx->sm_count * std::max(1, per_sm),
                                                   (int)std::min<long long>(spill_cap, 1 << 20))),
                             128, pair_smem, s>>>(pp);
     }

@@ -54,6 +54,16 @@ SIGNATURES = {
         _p, _p, _p, _p, c_int64, c_int64,
         c_double, c_double, c_int, c_float,
         _p, _p, _p, _p, _p, c_int64, _p, _p, _p]),
+    "cms_modified_cosine": (c_int, [
+        _p, _p, _p, _p, _p, _p, c_int64, c_int64,   # ctx, reference mz, a, b, off, precursor
+        _p, _p, _p, _p, _p, c_int64, c_int64,       # query mz, a, b, off, precursor
+        c_double, c_int,
+        _p, _p, _p, c_int64, _p, _p]),
+    "cms_modified_cosine_sparse": (c_int, [
+        _p, _p, _p, _p, _p, _p, c_int64, c_int64,
+        _p, _p, _p, _p, _p, c_int64, c_int64,
+        c_double, c_int, c_float,
+        _p, _p, _p, _p, _p, c_int64, _p, _p, _p]),
     "cms_cosine_greedy_noalloc": (c_int, [
         _p, _p, _p, _p, c_int64, c_int64,
         _p, _p, _p, _p, c_int64, c_int64,

@@ -217,3 +217,79 @@ def _fingerprint_matrix(measure: str, r_bits, r_valid, q_bits, q_valid, n_words:
                              int(out.stride(0)), stream_handle(s))
     check(rc, "cms_fingerprint")
     return out
+
+
+def modified_cosine_dense(ref: DeviceSpectra, ref_precursor, qry: DeviceSpectra, qry_precursor,
+                          tolerance: float, match_limit: int, *, out=None,
+                          config: Optional[dict] = None, stream=None,
+                          check_errors: bool = False):
+    """Modified cosine for all pairs -> (score f32, matches i32, overflow u8)
+    [n_ref, n_q]; *_precursor are device float64 tensors, one per spectrum."""
+    lib = _native.load()
+    device = ref.mz.device if ref.mz is not None else qry.mz.device
+    s = _stream(device, stream)
+    if out is None:
+        out = (torch.empty((ref.n, qry.n), dtype=torch.float32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.int32, device=device),
+               torch.empty((ref.n, qry.n), dtype=torch.uint8, device=device))
+    score, matches, overflow = out
+    ld = score.stride(0) if score.dim() == 2 else qry.n
+    ctx = _native.context(device.index)
+    cfg = _cfg(config)
+    rc = lib.cms_modified_cosine(
+        ctx.handle, ptr(ref.mz), ptr(ref.a), ptr(ref.b), ptr(ref.offsets), ptr(ref_precursor),
+        ref.n, ref.n_peaks, ptr(qry.mz), ptr(qry.a), ptr(qry.b), ptr(qry.offsets),
+        ptr(qry_precursor), qry.n, qry.n_peaks, float(tolerance), int(match_limit), ptr(score),
+        ptr(matches), ptr(overflow), int(ld), None if cfg is None else _ctypes_ref(cfg),
+        stream_handle(s))
+    check(rc, "cms_modified_cosine")
+    if check_errors:
+        bits = ctx.take_device_error(stream_handle(s))
+        if bits & _native.DEVERR_SPILL_OVERRUN and not (config or {}).get("mode") == 2:
+            return modified_cosine_dense(ref, ref_precursor, qry, qry_precursor, tolerance,
+                                         match_limit, out=out, config=dict(config or {}, mode=2),
+                                         stream=stream, check_errors=True)
+        if bits & _native.DEVERR_SPECTRUM_TOO_LONG:
+            raise NativeError("cms_modified_cosine: a spectrum has more than 32767 peaks",
+                              _native.CMS_ERR_DEVICE)
+        _raise_device_error(bits, "cms_modified_cosine")
+    return score, matches, overflow
+
+
+def modified_cosine_sparse(ref: DeviceSpectra, ref_precursor, qry: DeviceSpectra, qry_precursor,
+                           tolerance: float, match_limit: int, threshold: float, *,
+                           capacity: Optional[int] = None, config: Optional[dict] = None,
+                           stream=None) -> SparseHits:
+    """Modified-cosine pairs with score >= threshold (> 0); synchronises."""
+    lib = _native.load()
+    device = ref.mz.device if ref.mz is not None else qry.mz.device
+    s = _stream(device, stream)
+    ctx = _native.context(device.index)
+    cap = int(capacity) if capacity else max(1024, min(ref.n * qry.n, 1 << 22))
+    count = torch.zeros(1, dtype=torch.int64, device=device)
+    while True:
+        cfg = _cfg(config)
+        bufs = (torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.float32, device=device),
+                torch.empty(cap, dtype=torch.int32, device=device),
+                torch.empty(cap, dtype=torch.uint8, device=device))
+        rc = lib.cms_modified_cosine_sparse(
+            ctx.handle, ptr(ref.mz), ptr(ref.a), ptr(ref.b), ptr(ref.offsets), ptr(ref_precursor),
+            ref.n, ref.n_peaks, ptr(qry.mz), ptr(qry.a), ptr(qry.b), ptr(qry.offsets),
+            ptr(qry_precursor), qry.n, qry.n_peaks, float(tolerance), int(match_limit),
+            float(threshold), *[ptr(b) for b in bufs], cap, ptr(count),
+            None if cfg is None else _ctypes_ref(cfg), stream_handle(s))
+        check(rc, "cms_modified_cosine_sparse")
+        bits = ctx.take_device_error(stream_handle(s))  # synchronises s
+        if bits & _native.DEVERR_SPILL_OVERRUN and not (config or {}).get("mode") == 2:
+            config = dict(config or {}, mode=2)
+            continue
+        if bits & _native.DEVERR_SPECTRUM_TOO_LONG:
+            raise NativeError("cms_modified_cosine_sparse: a spectrum has more than 32767 peaks",
+                              _native.CMS_ERR_DEVICE)
+        _raise_device_error(bits, "cms_modified_cosine_sparse")
+        n = int(count.item())
+        if n <= cap:
+            return SparseHits(*bufs, n)
+        cap = n

@@ -218,6 +218,41 @@ int cms_cosine_greedy_sparse(cms_ctx* ctx, const float* ref_mz, const double* re
                              void* stream);
 
 /*
+ * Modified cosine (matchms ModifiedCosine): greedy cosine over the union of
+ * the matches at shift 0 and the matches at the pair's precursor difference
+ * shift = ref_precursor[i] - q_precursor[j] (precursor m/z per spectrum,
+ * device float64), in matchms' order -- the unshifted candidates, then the
+ * shifted ones, each generated reference-peak-major; one stable descending
+ * sort of the keys over that concatenation, one greedy.  No CUDA counterpart
+ * in the reference: it prototypes ModifiedCosine beside its CUDA classes
+ * (notebooks/prototyping/other_similarities.ipynb) and carries the shift it
+ * needs in its kernel (spectrum_similarity_functions.py:14,133).  Outputs,
+ * match_limit (counted over the concatenation), overflow, cfg and the sparse
+ * form follow cms_cosine_greedy / cms_cosine_greedy_sparse; spectra may have
+ * at most 32767 peaks (more sets CMS_ERR_DEVICE's spectrum-too-long bit).
+ * The join runs a second sweep per reference chunk through a neutral-loss
+ * index (m/z - precursor of each query peak) and confirms each of its
+ * candidates with matchms' float64 shifted-window test.
+ */
+int cms_modified_cosine(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                        const double* ref_b, const int64_t* ref_off, const double* ref_precursor,
+                        int64_t n_ref, int64_t n_ref_peaks, const float* q_mz, const double* q_a,
+                        const double* q_b, const int64_t* q_off, const double* q_precursor,
+                        int64_t n_q, int64_t n_q_peaks, double tolerance, int match_limit,
+                        float* score, int32_t* matches, uint8_t* overflow, int64_t ld,
+                        const cms_cosine_config* cfg, void* stream);
+int cms_modified_cosine_sparse(cms_ctx* ctx, const float* ref_mz, const double* ref_a,
+                               const double* ref_b, const int64_t* ref_off,
+                               const double* ref_precursor, int64_t n_ref, int64_t n_ref_peaks,
+                               const float* q_mz, const double* q_a, const double* q_b,
+                               const int64_t* q_off, const double* q_precursor, int64_t n_q,
+                               int64_t n_q_peaks, double tolerance, int match_limit,
+                               float threshold, int32_t* hit_ref, int32_t* hit_query,
+                               float* hit_score, int32_t* hit_matches, uint8_t* hit_overflow,
+                               int64_t capacity, int64_t* hit_count, const cms_cosine_config* cfg,
+                               void* stream);
+
+/*
  * Resident library: a spectrum set indexed once on the device (the "reference"
  * side of matchms, e.g. a spectral library) and searched by many query
  * batches.  This is the served form of CudaCosineGreedy.matrix(library,
