@@ -422,10 +422,11 @@ struct Pool {
 //                            slot of the chain head | length << 12; runs of at
 //                            most kMidRun from the front, longer ones from the back
 //   x     float  [32]        per-lane sweeping-peak m/z (modified cosine's exact test)
+//   t0    uint64             %globaltimer at the current item's start (trace only)
 constexpr int kLongRuns = 64;
 __host__ __device__ constexpr int head_words(int tile) { return (((tile + 1) / 2) + 3) & ~3; }
 __host__ __device__ constexpr int warp_slice_bytes(int tile) {
-    return 16 * kPool + 4 * head_words(tile) + 8 * 32 + 8 * 32 + 4 * kLongRuns + 4 * 32;
+    return 16 * kPool + 4 * head_words(tile) + 8 * 32 + 8 * 32 + 4 * kLongRuns + 4 * 32 + 16;
 }
 
 // Reference peak of a candidate's generation word.  Modified cosine marks
@@ -527,6 +528,8 @@ join_kernel(JoinParams P) {
     float2* s_lh = reinterpret_cast<float2*>(slice + 16 * kPool + 4 * hw + 8 * 32);
     uint32_t* long_runs = reinterpret_cast<uint32_t*>(slice + 16 * kPool + 4 * hw + 16 * 32);
     float* s_x = reinterpret_cast<float*>(slice + 16 * kPool + 4 * hw + 16 * 32 + 4 * kLongRuns);
+    unsigned long long* s_t0 = reinterpret_cast<unsigned long long*>(
+        slice + 16 * kPool + 4 * hw + 16 * 32 + 4 * kLongRuns + 4 * 32);
     Pool pool;
     {
         const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
@@ -564,7 +567,7 @@ join_kernel(JoinParams P) {
             ai -= nA;
             ++tt;
         }
-        const unsigned long long t_item = P.trace.rec ? global_ns() : 0ull;
+        if (P.trace.rec && lane == 0) *s_t0 = global_ns();
         const int t = (int)tt;
         const int a = P.a_order[ai];
         const int64_t a0 = P.A.off[a];
@@ -624,60 +627,80 @@ join_kernel(JoinParams P) {
             // finds the peak that owns it by a binary search over the warp's
             // inclusive entry counts: every lane tests an entry in every
             // round, however unevenly the entries fall among the peaks.
+            // Latency is hidden by running ahead: a step's bucket-table loads
+            // are issued one step early (steps are chunks, or chunk x pass
+            // for modified cosine), the peaks a probe needs two chunks early,
+            // and the entries of two rounds are loaded before either is tested.
             int n = 0;  // candidates found (warp-uniform)
-            float nx_mz = 0.f;
-            double nx_w = 0.0;
-            if (lane < na) {
-                nx_mz = P.A.mz[a0 + lane];
-                nx_w = __dmul_rn(peak_a(P.A.a, a0 + lane), P.A.b[a0 + lane]);
-            }
-            for (int pc = 0; pc < na; pc += 32) {
+            constexpr int kPasses = MODIFIED ? 2 : 1;
+            const int n_steps = ((na + 31) >> 5) * kPasses;
+            float mz_c = 0.f, mz_n = 0.f, mz_nn = 0.f;  // chunks c, c+1, c+2
+            double w_c = 0.0, w_n = 0.0, w_nn = 0.0;
+            auto load_peak = [&](int pp, float& mz, double& w) {
+                if (pp < na) {
+                    mz = P.A.mz[a0 + pp];
+                    w = __dmul_rn(peak_a(P.A.a, a0 + pp), P.A.b[a0 + pp]);
+                }
+            };
+            load_peak(lane, mz_c, w_c);
+            load_peak(32 + lane, mz_n, w_n);
+            load_peak(64 + lane, mz_nn, w_nn);
+            // one step's window and raw bucket-table values (consumed a step later)
+            float pL = 1.0f, pH = 0.0f;
+            uint32_t pt0 = 0, pt1 = 0, pt2 = 0, pt3 = 0;
+            auto probe = [&](bool valid, float mz, bool shifted) {
+                pL = 1.0f;
+                pH = 0.0f;
+                pt0 = pt1 = pt2 = pt3 = 0u;
+                if (!valid) return;
+                const bool ok = (MODIFIED && shifted)
+                                    ? nl_window(mz, P.A.prec[a], P.tol, pL, pH)
+                                    : Window<A_IS_REF, NOSHIFT>::bounds(mz, P.tol, P.shift, pL, pH);
+                if (!ok) {
+                    atomicOr(P.err, kErrBadOffsets);
+                    pL = 1.0f;
+                    pH = 0.0f;
+                    return;
+                }
+                if (!(pL <= pH)) return;
+                const uint32_t* TT = (MODIFIED && shifted) ? T2 : T;
+                const long long blo = bucket_of(pL, P.g.inv_w);
+                const long long bhi = bucket_of(pH, P.g.inv_w);
+                if (bhi - blo + 1 >= P.g.nb) {
+                    pt0 = __ldg(&TT[0]);
+                    pt1 = __ldg(&TT[P.g.nb]);
+                } else {
+                    const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
+                    pt0 = __ldg(&TT[bl]);
+                    if (bl <= bh) {
+                        pt1 = __ldg(&TT[bh + 1]);
+                    } else {  // wrapped: [bl, nb) then [0, bh]
+                        pt1 = __ldg(&TT[P.g.nb]);
+                        pt2 = __ldg(&TT[0]);
+                        pt3 = __ldg(&TT[bh + 1]);
+                    }
+                }
+            };
+            probe(lane < na, mz_c, false);
+            for (int st = 0; st < n_steps; ++st) {
+                const int pass = MODIFIED ? (st & 1) : 0;
+                const int pc = (MODIFIED ? (st >> 1) : st) * 32;
                 const int p = pc + lane;
-                const float mzA = nx_mz;
-                const double wA = nx_w;
-                if (p + 32 < na) {
-                    nx_mz = P.A.mz[a0 + p + 32];
-                    nx_w = __dmul_rn(peak_a(P.A.a, a0 + p + 32), P.A.b[a0 + p + 32]);
+                // this step's probe
+                const float L = pL, H = pH;
+                const uint32_t r0b = pt0, c0 = pt1 - pt0, r1b = pt2, c1 = pt3 - pt2;
+                if (pass == 0) {
+                    s_wa[lane] = w_c;
+                    if (MODIFIED) s_x[lane] = mz_c;
                 }
-                s_wa[lane] = wA;
-                if (MODIFIED) s_x[lane] = mzA;
-                // modified cosine sweeps the chunk twice: at shift 0 through
-                // the m/z index, then at each query's precursor difference
-                // through the neutral-loss index
-#pragma unroll 1
-                for (int pass = 0; pass < (MODIFIED ? 2 : 1); ++pass) {
-                const uint32_t* TT = (MODIFIED && pass) ? T2 : T;
+                // the next step's probe, in flight during this step's rounds
+                if (st + 1 < n_steps) {
+                    if (MODIFIED && pass == 0)
+                        probe(p < na, mz_c, true);
+                    else
+                        probe(p + 32 < na, mz_n, false);
+                }
                 const Entry* EE = (MODIFIED && pass) ? P.ent2 : ent;
-                float L = 1.0f, H = 0.0f;
-                uint32_t r0b = 0, c0 = 0, r1b = 0, c1 = 0;
-                if (p < na) {
-                    const bool ok = (MODIFIED && pass)
-                                        ? nl_window(mzA, P.A.prec[a], P.tol, L, H)
-                                        : Window<A_IS_REF, NOSHIFT>::bounds(mzA, P.tol, P.shift, L, H);
-                    if (!ok) {
-                        atomicOr(P.err, kErrBadOffsets);
-                        L = 1.0f;
-                        H = 0.0f;
-                    }
-                    if (L <= H) {
-                        const long long blo = bucket_of(L, P.g.inv_w);
-                        const long long bhi = bucket_of(H, P.g.inv_w);
-                        if (bhi - blo + 1 >= P.g.nb) {
-                            r0b = __ldg(&TT[0]);
-                            c0 = __ldg(&TT[P.g.nb]) - r0b;
-                        } else {
-                            const unsigned bl = (unsigned)blo & nbmask, bh = (unsigned)bhi & nbmask;
-                            r0b = __ldg(&TT[bl]);
-                            if (bl <= bh) {
-                                c0 = __ldg(&TT[bh + 1]) - r0b;
-                            } else {
-                                c0 = __ldg(&TT[P.g.nb]) - r0b;
-                                r1b = __ldg(&TT[0]);
-                                c1 = __ldg(&TT[bh + 1]) - r1b;
-                            }
-                        }
-                    }
-                }
                 s_lh[lane] = make_float2(L, H);
                 const uint32_t c = c0 + c1;
                 uint32_t incl = c;
@@ -691,86 +714,105 @@ join_kernel(JoinParams P) {
                 const bool wrapped = __any_sync(full, c1 != 0u);
                 const uint32_t off0 = r0b - excl;  // entry k of lane l: r0b + (k - excl)
                 __syncwarp();
-                for (uint32_t kb = 0; kb < E; kb += 32) {
-                    const uint32_t k = kb + (uint32_t)lane;
-                    int o = 0;
+                // position of flat entry k, and the lane (peak) that owns it
+                auto locate = [&](uint32_t k, int& o) -> uint32_t {
+                    o = 0;
 #pragma unroll
                     for (int step = 16; step > 0; step >>= 1) {
                         const uint32_t v = __shfl_sync(full, incl, o + step - 1);
                         if (v <= k) o += step;
                     }
-                    uint32_t pos;
-                    if (!wrapped) {
-                        pos = __shfl_sync(full, off0, o & 31) + k;
-                    } else {
-                        const uint32_t oex = __shfl_sync(full, excl, o & 31);
-                        const uint32_t oc0 = __shfl_sync(full, c0, o & 31);
-                        const uint32_t or0 = __shfl_sync(full, r0b, o & 31);
-                        const uint32_t or1 = __shfl_sync(full, r1b, o & 31);
-                        const uint32_t e = k - oex;
-                        pos = e < oc0 ? or0 + e : or1 + (e - oc0);
+                    if (!wrapped) return __shfl_sync(full, off0, o & 31) + k;
+                    const uint32_t oex = __shfl_sync(full, excl, o & 31);
+                    const uint32_t oc0 = __shfl_sync(full, c0, o & 31);
+                    const uint32_t or0 = __shfl_sync(full, r0b, o & 31);
+                    const uint32_t or1 = __shfl_sync(full, r1b, o & 31);
+                    const uint32_t e = k - oex;
+                    return e < oc0 ? or0 + e : or1 + (e - oc0);
+                };
+                for (uint32_t kb = 0; kb < E; kb += 64) {
+                    // two rounds' entries in flight before either is tested
+                    int ow[2];
+                    Entry enb[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const uint32_t k = kb + 32u * u + (uint32_t)lane;
+                        const uint32_t pos = locate(k, ow[u]);
+                        enb[u].id = 0;
+                        if (k < E) enb[u] = EE[tbase + pos];
                     }
-                    bool cand = false;
-                    Entry en;
-                    en.id = 0;
-                    if (k < E) {
-                        en = EE[tbase + pos];
-                        const float2 lh = s_lh[o];
-                        const int bq = (int)(en.id >> 16);
-                        cand = en.mz >= lh.x && en.mz <= lh.y && bq >= range_lo && bq < range_hi;
-                        if (MODIFIED && pass && cand) {
-                            // the shifted window exactly as matchms tests it:
-                            // mz2 = mz_q + (prec_ref - prec_q) against mz_ref -+ tol
-                            const int qb = b_begin + bq;
-                            const float y = P.B.mz[P.B.off[qb] + (en.id & 0xFFFFu)];
-                            const double mz2 =
-                                __dadd_rn((double)y, __dsub_rn(P.A.prec[a], P.B.prec[qb]));
-                            const double x = (double)s_x[o];
-                            cand = !(mz2 > __dadd_rn(x, P.tol)) && !(mz2 < __dsub_rn(x, P.tol));
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        if (kb + 32u * u >= E) break;
+                        const uint32_t k = kb + 32u * u + (uint32_t)lane;
+                        const int o = ow[u];
+                        const Entry en = enb[u];
+                        bool cand = false;
+                        if (k < E) {
+                            const float2 lh = s_lh[o];
+                            const int bq = (int)(en.id >> 16);
+                            cand = en.mz >= lh.x && en.mz <= lh.y && bq >= range_lo && bq < range_hi;
+                            if (MODIFIED && pass && cand) {
+                                // the shifted window exactly as matchms tests it:
+                                // mz2 = mz_q + (prec_ref - prec_q) against mz_ref -+ tol
+                                const int qb = b_begin + bq;
+                                const float y = P.B.mz[P.B.off[qb] + (en.id & 0xFFFFu)];
+                                const double mz2 =
+                                    __dadd_rn((double)y, __dsub_rn(P.A.prec[a], P.B.prec[qb]));
+                                const double x = (double)s_x[o];
+                                cand = !(mz2 > __dadd_rn(x, P.tol)) && !(mz2 < __dsub_rn(x, P.tol));
+                            }
                         }
-                    }
-                    const unsigned bal = __ballot_sync(full, cand);
-                    const int slot = n + __popc(bal & below);
-                    n += __popc(bal);
-                    if (cand && slot < P.pool_max) {
-                        const int bq = (int)(en.id >> 16);
-                        const int pB = (int)(en.id & 0xFFFFu);
-                        const int pa = pc + o;
-                        const double aB = P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
-                        double key;
-                        uint32_t gen;
-                        if (A_IS_REF) {
-                            key = __dmul_rn(__dmul_rn(s_wa[o], aB), en.b);
-                            gen = ((uint32_t)pa << 16) | (uint32_t)pB;
-                            if (MODIFIED) gen |= (uint32_t)pass << 31;
-                        } else {
-                            const double wB = __dmul_rn(aB, en.b);
-                            key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + pa)), P.A.b[a0 + pa]);
-                            gen = ((uint32_t)pB << 16) | (uint32_t)pa;
+                        const unsigned bal = __ballot_sync(full, cand);
+                        const int slot = n + __popc(bal & below);
+                        n += __popc(bal);
+                        if (cand && slot < P.pool_max) {
+                            const int bq = (int)(en.id >> 16);
+                            const int pB = (int)(en.id & 0xFFFFu);
+                            const int pa = pc + o;
+                            const double aB = P.B.a ? P.B.a[P.B.off[b_begin + bq] + pB] : 1.0;
+                            double key;
+                            uint32_t gen;
+                            if (A_IS_REF) {
+                                key = __dmul_rn(__dmul_rn(s_wa[o], aB), en.b);
+                                gen = ((uint32_t)pa << 16) | (uint32_t)pB;
+                                if (MODIFIED) gen |= (uint32_t)pass << 31;
+                            } else {
+                                const double wB = __dmul_rn(aB, en.b);
+                                key = __dmul_rn(__dmul_rn(wB, peak_a(P.A.a, a0 + pa)),
+                                                P.A.b[a0 + pa]);
+                                gen = ((uint32_t)pB << 16) | (uint32_t)pa;
+                            }
+                            // push onto the query's chain: swap the new slot into
+                            // its 16-bit head; the old head, if of this epoch, is
+                            // the chain's next element
+                            const int qr = bq - range_lo;
+                            uint32_t* hp = head + (qr >> 1);
+                            const unsigned sh = (unsigned)(qr & 1) * 16u;
+                            const unsigned nh = (epoch << 12) | (unsigned)slot;
+                            unsigned cur = *reinterpret_cast<volatile uint32_t*>(hp), assumed, ph;
+                            do {
+                                assumed = cur;
+                                ph = (assumed >> sh) & 0xFFFFu;
+                                cur = atomicCAS(hp, assumed,
+                                                (assumed & ~(0xFFFFu << sh)) | (nh << sh));
+                            } while (cur != assumed);
+                            uint32_t m = (uint32_t)qr;
+                            if ((ph >> 12) == epoch) m |= ((ph & 0xFFFu) << 12) | kHasNext;
+                            pool.put(slot, key, gen, m);
                         }
-                        // push onto the query's chain: swap the new slot into
-                        // its 16-bit head; the old head, if of this epoch, is
-                        // the chain's next element
-                        const int qr = bq - range_lo;
-                        uint32_t* hp = head + (qr >> 1);
-                        const unsigned sh = (unsigned)(qr & 1) * 16u;
-                        const unsigned nh = (epoch << 12) | (unsigned)slot;
-                        unsigned cur = *reinterpret_cast<volatile uint32_t*>(hp), assumed, ph;
-                        do {
-                            assumed = cur;
-                            ph = (assumed >> sh) & 0xFFFFu;
-                            cur = atomicCAS(hp, assumed, (assumed & ~(0xFFFFu << sh)) | (nh << sh));
-                        } while (cur != assumed);
-                        uint32_t m = (uint32_t)qr;
-                        if ((ph >> 12) == epoch) m |= ((ph & 0xFFFu) << 12) | kHasNext;
-                        pool.put(slot, key, gen, m);
                     }
                     if (n > P.pool_max) break;
                 }
-                __syncwarp();  // s_lh / s_wa / s_x are rewritten by the next pass or chunk
+                __syncwarp();  // s_lh / s_wa / s_x are rewritten by the next step
                 if (n > P.pool_max) break;
+                if (pass == kPasses - 1) {  // next chunk: rotate the prefetched peaks
+                    mz_c = mz_n;
+                    w_c = w_n;
+                    mz_n = mz_nn;
+                    w_n = w_nn;
+                    load_peak(pc + 96 + lane, mz_nn, w_nn);
                 }
-                if (n > P.pool_max) break;
             }
             __syncwarp();
             if (n > P.pool_max) {
@@ -1049,7 +1091,7 @@ join_kernel(JoinParams P) {
                 unsigned long long* r = P.trace.rec + 4 * k;
                 r[0] = (unsigned long long)P.trace.tag | ((unsigned long long)smid << 32);
                 r[1] = base + (unsigned long long)f;
-                r[2] = t_item;
+                r[2] = *s_t0;
                 r[3] = global_ns();
             }
         }
