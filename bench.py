@@ -307,10 +307,14 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(dev)
     ref, qry = make_data(args, rank)
     cfg = json.loads(args.config) if args.config else None
+    tune_report = None
     if cfg is None:
         from cudams import autotune
 
-        cfg = autotune.choose_config(ref, qry, TOL)
+        # timed trials on a sample of this workload: tile, then per peak-count
+        # bucket of the reference spectra the first sub-range width
+        cfg, tune_report = autotune.measure(ref, qry, TOL, 0.0, MATCH_LIMIT, device=dev,
+                                            record=False)
     rd, qd = ref.to_device(dev), qry.to_device(dev)
     R, Q = ref.n, qry.n
     free, _ = torch.cuda.mem_get_info(dev)
@@ -399,7 +403,15 @@ def run_ours(args, world, rank, local):
             "data": "synthetic (seeded; stands in for GNPS)",
             "config": {"workload": WORKLOAD, "n_ref_per_rank": R, "n_query": Q,
                        "pairs_per_step_per_rank": R * Q, "row_blocks": len(blocks),
-                       "tuning": cfg, "l2": "inputs larger than L2 (no flush)",
+                       "tuning": cfg,
+                       "tuning_measured": None if tune_report is None else {
+                           "seconds": tune_report["seconds"],
+                           "heuristic": tune_report["heuristic"],
+                           "tile_trials_ms": {str(t["tile_spectra"]): round(t["ms"], 4)
+                                              for t in tune_report["trials"]
+                                              if "tile_spectra" in t},
+                           "buckets": tune_report["buckets"]},
+                       "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"row shards x{world}, no collective"},
             "gpu_launches": int(stage_n.sum()),
             "roofline": roofline, "clocks": clk}

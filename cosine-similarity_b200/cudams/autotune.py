@@ -221,9 +221,11 @@ class Tuner:
             torch.cuda.synchronize()
             return e0.elapsed_time(e1) / reps
 
-        # 1) tile size: the estimate and its neighbours
+        # 1) tile size: the estimate and its neighbours (at most MAX_AUTO_TILE:
+        # larger tiles cost the join a CTA per SM)
         t0 = base["tile_spectra"]
-        tiles = sorted({max(32, min(4096, (t + 31) // 32 * 32)) for t in (t0 // 2, t0, 2 * t0)})
+        tiles = sorted({max(32, min(MAX_AUTO_TILE, (int(t) + 31) // 32 * 32))
+                        for t in (t0 / 2, 0.75 * t0, t0, 1.5 * t0, 2 * t0)})
         best_tile, best_ms = t0, float("inf")
         for t in tiles:
             ms = timed(rd, rs.n, dict(base, tile_spectra=t))
