@@ -14,7 +14,7 @@
 //                        first (log2 length classes), for load balance
 //   4. index kernels     query spectra are cut into tiles of tile_spectra;
 //                        each tile's peaks are bucketed by m/z (bucket width
-//                        >= 2*tol, buckets hashed modulo n_buckets) into a
+//                        tol by default, buckets hashed modulo n_buckets) into a
 //                        CSR "tile stream" of (m/z, query<<16 | peak)
 //   5. join_kernel       persistent warps; one work item = (reference
 //                        spectrum, query tile).  Lanes take reference peaks,
@@ -584,8 +584,7 @@ join_kernel(JoinParams P) {
             __stcs(&P.dense.score[o], sc);
             __stcs(&P.dense.matches[o], mt);
         };
-        auto store_result = [&](int bq, double score, int mt) {
-            const double snB = P.snB[bq];
+        auto store_result_n = [&](int bq, double score, int mt, double snB) {
             const float sc =
                 (float)__ddiv_rn(score, A_IS_REF ? __dmul_rn(snA, snB) : __dmul_rn(snB, snA));
             if (SPARSE) {
@@ -594,6 +593,9 @@ join_kernel(JoinParams P) {
             } else {
                 put_dense(bq, sc, mt);
             }
+        };
+        auto store_result = [&](int bq, double score, int mt) {
+            store_result_n(bq, score, mt, P.snB[bq]);
         };
 
         int width = tn;
@@ -988,6 +990,7 @@ join_kernel(JoinParams P) {
                 const int s = c + lane;
                 bool own = false;
                 int L = 0, qr = 0;
+                double snB_own = 0.0;
                 double k0 = 0.0, k1 = 0.0, k2 = 0.0;
                 uint32_t g0 = 0, g1 = 0, g2 = 0;
                 if (s < n) {
@@ -996,6 +999,8 @@ join_kernel(JoinParams P) {
                     const unsigned h = (head[qr >> 1] >> ((qr & 1) * 16)) & 0xFFFu;
                     own = h == (unsigned)s;
                     if (own) {
+                        // the query norm's load starts before the chain walk
+                        snB_own = P.snB[b_begin + range_lo + qr];
                         k0 = pool.key(s);
                         g0 = pool.gen(s);
                         L = 1;
@@ -1072,7 +1077,7 @@ join_kernel(JoinParams P) {
                                 ++mt;
                             }
                         }
-                        store_result(bq, score, mt);
+                        store_result_n(bq, score, mt, snB_own);
                     }
                 }
             }
@@ -1488,8 +1493,10 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
     }
     p.tile = (int)std::min<int64_t>(p.tile, std::max<int64_t>(1, args.qry.n));
     p.n_tiles = (int)((args.qry.n + p.tile - 1) / p.tile);
-    double w = (cfg && cfg->bucket_width > 0.0) ? cfg->bucket_width : 2.0 * args.tol;
-    if (w < args.tol) w = args.tol;
+    // bucket width: tol by default (a window spans two or three buckets);
+    // any width is correct, narrower ones want more buckets per tile
+    double w = (cfg && cfg->bucket_width > 0.0) ? cfg->bucket_width : args.tol;
+    if (w < 0.25 * args.tol) w = 0.25 * args.tol;
     if (!(w > 0.0)) w = 1e-3;
     p.width = w;
     const double avg_tile_peaks =

@@ -2,29 +2,24 @@
 //
 // Replaces cudams/similarity/vector_similarity_functions.py:12-119, which
 // computes I = R @ Q^T as a dense float32 GEMM over 0/1 values and then runs
-// four elementwise passes.  Here each 128 x 128 output tile is one CTA:
-//   - the 128 reference and 128 query rows of one K-chunk (up to 32 64-bit
-//     words = 2048 bits) are staged in shared memory (rows padded to 33 words
-//     so the column-strided reads of a warp hit 32 distinct banks);
-//   - each thread owns an 8 x 8 micro-tile: per 64-bit word it loads 8 + 8
-//     words and issues 64 AND + POPC pairs into integer accumulators (the
-//     popcount runs on the integer pipe; there is no floating point until
-//     the epilogue);
-//   - the epilogue forms the measure in IEEE float32 in the reference's
-//     order of operations and maps 0/0 to 0 (nan_to_num), or writes `fill`
-//     for rows/columns without a fingerprint.
+// four elementwise passes.  Here the intersection counts I come from the
+// tensor cores as an exact int8 GEMM over 0/1 bytes (tcgen05, int32
+// accumulators in TMEM), the row bit counts from popcounts of the packed
+// words, and the epilogue forms the measure in IEEE float32 in the
+// reference's order of operations, mapping 0/0 to 0 (nan_to_num), or writes
+// `fill` for rows/columns without a fingerprint.  The kernel is described
+// below, above namespace umma.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <cstring>
+#include <mutex>
 
 #include "cms_internal.cuh"
 
 namespace cms {
 namespace {
-
-constexpr int kBM = 128;
-constexpr int kBN = 128;
-constexpr int kKC = 32;          // 64-bit words per K chunk
-constexpr int kLd = kKC + 1;     // padded row stride (words)
-constexpr int kFpThreads = 256;  // 16 x 16 threads, 8 x 8 pairs each
 
 struct FpParams {
     const uint32_t* r;
@@ -39,13 +34,6 @@ struct FpParams {
     int64_t ld;
     int sym;  // only outputs (i, j) with i <= j (n_r == n_q)
 };
-
-__device__ __forceinline__ uint64_t load_word64(const uint32_t* row, int w64, int n_words) {
-    const int w = 2 * w64;
-    const uint32_t lo = w < n_words ? row[w] : 0u;
-    const uint32_t hi = (w + 1) < n_words ? row[w + 1] : 0u;
-    return (uint64_t)lo | ((uint64_t)hi << 32);
-}
 
 template <int MEASURE>
 __device__ __forceinline__ float measure_of(int inter, int a, int b) {
@@ -93,7 +81,7 @@ constexpr int kBM = 128;           // reference rows per tile (TMEM lanes)
 constexpr int kBN = 256;           // query rows per tile (accumulator columns)
 constexpr int kBKBytes = 128;      // expanded K bytes per stage (one 128B swizzle row)
 constexpr int kBKWords = kBKBytes / 32;  // packed uint32 words per row per stage
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kABytes = kBM * kBKBytes;  // 16 KB
 constexpr int kBBytes = kBN * kBKBytes;  // 32 KB
 constexpr int kStageBytes = kABytes + kBBytes;
@@ -106,7 +94,11 @@ constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
 
 // shared-memory layout (offsets from a 1024-byte aligned base)
 constexpr int kOffStages = 0;
-constexpr int kOffPop = kStages * kStageBytes;  // int pa[2][128], pb[2][256]
+// per epilogue warp: one 32 x 32 float chunk of the output, staged for a
+// tensor store (128-byte swizzle: 16-byte piece j of row r at j ^ (r % 8))
+constexpr int kStgBytes = 32 * 32 * 4;
+constexpr int kOffStg = kStages * kStageBytes;
+constexpr int kOffPop = kOffStg + kEpiWarps * kStgBytes;  // int pa[2][128], pb[2][256]
 constexpr int kOffBar = kOffPop + 2 * (kBM + kBN) * 4;
 // barriers: full[S], empty[S], tfull[2], tempty[2], pfull[2], pempty[2], done
 constexpr int kNumBars = 2 * kStages + 9;
@@ -201,6 +193,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 2-D tensor store of one staged chunk (box 32 x 32 floats at column x, row
+// y; elements outside the output are not written), and its completion
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(x), "r"(y), "r"(src)
+        : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 struct Geometry {
     int n_tm, n_tn;       // tiles along the reference / query side
     int64_t n_tiles;
@@ -250,7 +259,10 @@ __device__ __forceinline__ void expand_row(unsigned char* stage, int r, uint4 bi
 
 template <int MEASURE>
 __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geometry G,
-                                                               uint32_t* err) {
+                                                               uint32_t* err,
+                                                               const __grid_constant__ CUtensorMap
+                                                                   out_map,
+                                                               int use_map) {
     extern __shared__ unsigned char smem_dyn[];
     unsigned char* sm = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
@@ -400,6 +412,7 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
         const int quarter = warp & 3;        // TMEM lanes 32*quarter .. +31
         const int half = warp >> 2;          // columns 128*half .. +127
         const bool vec_out = (P.ld & 3) == 0 && (reinterpret_cast<uintptr_t>(P.out) & 15) == 0;
+        unsigned char* stg = sm + kOffStg + warp * kStgBytes;
         int64_t it = 0;
         for (int64_t t = blockIdx.x; t < G.n_tiles; t += gridDim.x) {
             int tm, tn;
@@ -420,7 +433,13 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
                 uint32_t v[32];
                 __syncwarp();
                 tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kBN + col_l), v);
-                if (gr < P.n_r && gc0 < P.n_q) {
+                // a chunk inside the tensor map's columns is stored by the
+                // warp (rows past the end hold the fill value and are clipped
+                // by the store); the others lane by lane
+                const bool tma_chunk = use_map && gc0 + 32 <= (P.n_q & ~int64_t(3));
+                const bool live = tma_chunk ? (int64_t)tm * kBM + quarter * 32 < P.n_r
+                                            : (gr < P.n_r && gc0 < P.n_q);
+                if (live) {
                     float o[32];
                     const int4* pbv = reinterpret_cast<const int4*>(pb + acc * kBN + col_l);
 #pragma unroll
@@ -435,10 +454,26 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
                                        : P.fill;
                         }
                     }
-                    // a lane writes 32 consecutive floats of its row: eight
-                    // 16-byte streaming stores when the chunk is whole, aligned
-                    // and (under sym) on or above the diagonal, else one by one
-                    if (vec_out && gc0 + 32 <= P.n_q && !(P.sym && gr > gc0)) {
+                    // with the output's tensor map: the warp stages its 32 x 32
+                    // chunk and one lane stores it (under sym, elements below
+                    // the diagonal are rewritten by the mirror pass anyway).
+                    // Else a lane writes 32 consecutive floats of its row:
+                    // eight 16-byte streaming stores when the chunk is whole,
+                    // aligned and (under sym) on or above the diagonal, else
+                    // one by one.
+                    if (tma_chunk) {
+                        if (lane == 0) tma_store_wait_read();  // the previous chunk left stg
+                        __syncwarp();
+#pragma unroll
+                        for (int j4 = 0; j4 < 8; ++j4)
+                            *reinterpret_cast<float4*>(stg + lane * 128 + ((j4 ^ (lane & 7)) << 4)) =
+                                make_float4(o[4 * j4], o[4 * j4 + 1], o[4 * j4 + 2], o[4 * j4 + 3]);
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0)
+                            tma_store_2d(&out_map, smem_u32(stg), (int)gc0,
+                                         (int)((int64_t)tm * kBM + quarter * 32));
+                    } else if (vec_out && gc0 + 32 <= P.n_q && !(P.sym && gr > gc0)) {
 #pragma unroll
                         for (int j4 = 0; j4 < 8; ++j4)
                             __stcs(reinterpret_cast<float4*>(orow + gc0) + j4,
@@ -458,6 +493,8 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
             mbar_arrive(&tempty[acc]);
             mbar_arrive(&pempty[acc]);
         }
+        if (use_map && lane == 0) tma_store_wait_all();
+        __syncwarp();
     }
 
     __syncthreads();
@@ -471,116 +508,60 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
 
 }  // namespace umma
 
-template <int MEASURE>
-__global__ void __launch_bounds__(kFpThreads)
-fingerprint_kernel(FpParams P) {
-    // symmetric: tiles wholly below the diagonal are copied afterwards
-    if (P.sym && blockIdx.y > blockIdx.x) return;
-    extern __shared__ __align__(16) uint64_t fp_smem[];
-    uint64_t* sR = fp_smem;
-    uint64_t* sQ = fp_smem + kBM * kLd;
-    __shared__ int pa[kBM];
-    __shared__ int pb[kBN];
-
-    const int tid = threadIdx.x;
-    const int tr = tid >> 4, tc = tid & 15;
-    const int64_t row0 = (int64_t)blockIdx.y * kBM;
-    const int64_t col0 = (int64_t)blockIdx.x * kBN;
-    const int n64 = (P.n_words + 1) >> 1;
-
-    int acc[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0;
-    if (tid < kBM) pa[tid] = 0;
-    if (tid >= kBM && tid < kBM + kBN) pb[tid - kBM] = 0;
-
-    for (int k0 = 0; k0 < n64; k0 += kKC) {
-        const int kc = min(kKC, n64 - k0);
-        __syncthreads();
-        // stage rows of this K chunk (zeros beyond the matrix edge)
-        for (int e = tid; e < kBM * kKC; e += kFpThreads) {
-            const int rr = e / kKC, k = e - rr * kKC;
-            const int64_t gr = row0 + rr;
-            uint64_t v = 0;
-            if (gr < P.n_r && k < kc) v = load_word64(P.r + gr * P.n_words, k0 + k, P.n_words);
-            sR[rr * kLd + k] = v;
-        }
-        for (int e = tid; e < kBN * kKC; e += kFpThreads) {
-            const int cc = e / kKC, k = e - cc * kKC;
-            const int64_t gc = col0 + cc;
-            uint64_t v = 0;
-            if (gc < P.n_q && k < kc) v = load_word64(P.q + gc * P.n_words, k0 + k, P.n_words);
-            sQ[cc * kLd + k] = v;
-        }
-        __syncthreads();
-        // row popcounts of this chunk
-        if (tid < kBM) {
-            int c = 0;
-            for (int k = 0; k < kc; ++k) c += __popcll(sR[tid * kLd + k]);
-            pa[tid] += c;
-        } else if (tid < kBM + kBN) {
-            const int cc = tid - kBM;
-            int c = 0;
-            for (int k = 0; k < kc; ++k) c += __popcll(sQ[cc * kLd + k]);
-            pb[cc] += c;
-        }
-        // AND + POPC over the chunk
-        for (int k = 0; k < kc; ++k) {
-            uint64_t rw[8], qw[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) rw[i] = sR[(tr + 16 * i) * kLd + k];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) qw[j] = sQ[(tc + 16 * j) * kLd + k];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] += __popcll(rw[i] & qw[j]);
-        }
-    }
-    __syncthreads();
-
-    // epilogue
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int rr = tr + 16 * i;
-        const int64_t gr = row0 + rr;
-        if (gr >= P.n_r) continue;
-        const bool rv = P.r_valid ? P.r_valid[gr] != 0 : true;
-        float* orow = P.out + gr * P.ld;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int cc = tc + 16 * j;
-            const int64_t gc = col0 + cc;
-            if (gc >= P.n_q || (P.sym && gr > gc)) continue;
-            const bool qv = P.q_valid ? P.q_valid[gc] != 0 : true;
-            orow[gc] = (rv && qv) ? measure_of<MEASURE>(acc[i][j], pa[rr], pb[cc]) : P.fill;
-        }
-    }
-}
-
 // Error bits of the tensor-core kernel (a pipeline wait that ran out of
 // time); read and cleared by cms_fingerprint_take_error.
 __device__ uint32_t g_fp_error;
 
 template <int MEASURE>
 int launch_umma(int grid, cudaStream_t s, const FpParams& P, const umma::Geometry& G,
-                uint32_t* err) {
+                uint32_t* err, const CUtensorMap& out_map, int use_map) {
     auto* k = umma::fp_umma_kernel<MEASURE>;
     if (const int rc = raise_func_smem(reinterpret_cast<const void*>(k), umma::kSmemBytes))
         return rc;
-    k<<<grid, umma::kThreads, umma::kSmemBytes, s>>>(P, G, err);
+    k<<<grid, umma::kThreads, umma::kSmemBytes, s>>>(P, G, err, out_map, use_map);
     return CMS_OK;
 }
 
-template <int MEASURE>
-int launch_fp(dim3 grid, size_t smem, cudaStream_t s, const FpParams& P) {
-    if (const int rc = raise_func_smem(reinterpret_cast<const void*>(fingerprint_kernel<MEASURE>),
-                                       smem))
-        return rc;
-    fingerprint_kernel<MEASURE><<<grid, kFpThreads, smem, s>>>(P);
-    return CMS_OK;
+// cuTensorMapEncodeTiled from the driver (through the runtime, so that the
+// library needs no link against libcuda); null when the driver lacks it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// Tensor map of the float output for the epilogue's 32 x 32 tensor stores:
+// n_r rows, row pitch ld, and the first n_q rounded down to a multiple of four
+// columns (a tensor store clips rows at the end, but columns only to whole 16
+// bytes, so the last partial group is stored lane by lane).  False when the
+// output does not meet the tensor-store rules (16-byte aligned base and
+// pitch), is narrower than four columns, or the driver has no encoder; the
+// epilogue then stores from registers.
+bool output_tensor_map(float* out, int64_t n_r, int64_t n_q, int64_t ld, CUtensorMap& map) {
+    std::memset(&map, 0, sizeof(map));
+    const int64_t n_q4 = n_q & ~int64_t(3);
+    if ((reinterpret_cast<uintptr_t>(out) & 15) || (ld & 3) || n_q4 == 0 ||
+        n_q > (1LL << 31) || n_r > (1LL << 31))
+        return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)n_q4, (cuuint64_t)n_r};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, out, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -619,16 +600,18 @@ int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
     uint32_t* err = nullptr;
     CMS_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&err), g_fp_error));
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sms, G.n_tiles));
+    CUtensorMap out_map;
+    const int use_map = output_tensor_map(out, n_ref, n_q, ld, out_map) ? 1 : 0;
     int rc = CMS_OK;
     switch (measure) {
         case CMS_FP_JACCARD:
-            rc = launch_umma<CMS_FP_JACCARD>(grid, s, P, G, err);
+            rc = launch_umma<CMS_FP_JACCARD>(grid, s, P, G, err, out_map, use_map);
             break;
         case CMS_FP_DICE:
-            rc = launch_umma<CMS_FP_DICE>(grid, s, P, G, err);
+            rc = launch_umma<CMS_FP_DICE>(grid, s, P, G, err, out_map, use_map);
             break;
         default:
-            rc = launch_umma<CMS_FP_COSINE>(grid, s, P, G, err);
+            rc = launch_umma<CMS_FP_COSINE>(grid, s, P, G, err, out_map, use_map);
             break;
     }
     if (rc) return rc;

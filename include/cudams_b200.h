@@ -142,8 +142,10 @@ int cms_cosine_greedy_plain(const float* ref_mz, const double* ref_a, const doub
 /*
  * Tuning of the tiled path.  Zero in a field means "choose automatically".
  *   tile_spectra   query spectra per indexed tile (<= 4096)
- *   bucket_width   m/z width of one index bucket (>= tolerance)
- *   n_buckets      buckets per tile (power of two)
+ *   bucket_width   m/z width of one index bucket (default: the tolerance;
+ *                  at least a quarter of it)
+ *   n_buckets      buckets per tile (power of two; default: the tile's peak
+ *                  count rounded up, at least 1024)
  *   mode           0 auto, 1 indexed join with pair spill, 2 pair kernel only
  *   pair_threads   threads per CTA of the pair kernel (64..512, multiple of 32)
  *   cand_per_pair  expected candidates per pair (e.g. sampled on the host);

@@ -136,6 +136,42 @@ def test_pair_kernel_register_sort(cuda_device, ml, threads):
     assert_same(gpu_dense(ref, qry2, p, {"mode": 2}), want, f"ml {ml} auto threads")
 
 
+def _block_spectra(n, seed, levels):
+    """Spectra of 50 tight groups of 20 peaks (every peak of a group within
+    0.01 of the others) with intensities drawn from `levels`: one intensity
+    level gives all-equal keys, ordered by generation alone."""
+    from cudams.packing import PackedSpectra
+
+    rng = np.random.default_rng(seed)
+    centres = 100.0 + 10.0 * np.arange(50)
+    mz, b, off = [], [], [0]
+    for _ in range(n):
+        m = np.sort((np.repeat(centres, 20) + rng.uniform(-0.004, 0.004, 1000)).astype(np.float32))
+        mz.append(m)
+        b.append(rng.choice(np.asarray(levels, np.float64), m.shape[0]))
+        off.append(off[-1] + m.shape[0])
+    return PackedSpectra(np.concatenate(mz), None, np.concatenate(b),
+                         np.asarray(off, np.int64), 0.0, 1.0, 2048)
+
+
+@pytest.mark.parametrize("levels", [[1.0], [0.25, 0.5, 1.0], None])
+@pytest.mark.parametrize("ml", [1024, 2048])
+def test_pair_kernel_equal_keys(cuda_device, levels, ml):
+    """Blocks of 20 x 20 candidates per peak group with all-equal keys (the
+    order is generation alone), a few intensity levels (many ties broken by
+    generation) or distinct keys (None): bit-exact through the whole-matrix
+    pair kernel (register and shared-memory sorts) and through spills."""
+    lv = levels if levels is not None else list(np.linspace(0.01, 1.0, 997))
+    ref = _block_spectra(5, 30 + ml, lv)
+    qry = _block_spectra(4, 40 + ml, lv)
+    p = P(0.01, ml, 2048)
+    want = oracle.cosine_greedy(ref, qry, 0.01, 0.0, ml)
+    assert want[2].mean() > 0.5
+    assert_same(gpu_dense(ref, qry, p, {"mode": 2}), want, f"mode2 {levels}")
+    assert_same(gpu_dense(ref, qry, p, {"mode": 2, "pair_threads": 64}), want, f"64 {levels}")
+    assert_same(gpu_dense(ref, qry, p, {"mode": 1, "tile_spectra": 32}), want, f"spill {levels}")
+
+
 def test_self_similarity_spills(cuda_device):
     """Identical sets: diagonal pairs have one candidate per peak (long runs ->
     pair kernel), off-diagonal pairs few; both paths must agree."""

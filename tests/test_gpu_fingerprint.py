@@ -163,3 +163,28 @@ def test_symmetric_class_api(cuda_device):
     _bits_equal(sym, full)
     with pytest.raises(ValueError, match="is_symmetric"):
         sim.matrix(spectra, spectra[:-1], is_symmetric=True)
+
+
+@pytest.mark.parametrize("ld", [517, 520, 640])  # 520, 640: tensor-store path; 517: per-lane stores
+@pytest.mark.parametrize("measure", MEASURES)
+def test_output_pitch(cuda_device, measure, ld):
+    """Results land in an output with row pitch ld >= n_q (ragged tiles on both
+    sides); the columns between n_q and ld keep their contents."""
+    import torch
+
+    from cudams import kernels, synthetic
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    nr, nq, n_words = 300, 517, 64
+    a = synthetic.fingerprints(nr, seed=21)
+    b = synthetic.fingerprints(nq, seed=22)
+    va = np.ones(nr, np.uint8)
+    va[299] = 0
+    buf = torch.full((nr, ld), 7.0, dtype=torch.float32, device=dev)
+    out = buf[:, :nq]
+    kernels.fingerprint_matrix(measure, t(a), t(va), t(b), None, n_words, np.nan, out=out,
+                               check_errors=True)
+    host = buf.cpu().numpy()
+    _bits_equal(host[:, :nq], oracle.fingerprint(measure, a, va, b, None, n_words, np.nan))
+    assert (host[:, nq:] == 7.0).all()
