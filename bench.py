@@ -24,9 +24,15 @@ Multi-GPU (torchrun): each rank computes its own 100k-reference shard against
 the same queries; no collective on the data path ("scaling": "weak").
 
 --impl reference times the reference's CPU implementation of the path: the
-reference is a Python/Numba package whose GPU kernel cannot be built here,
-so its CPU restatement (oracle/, C + OpenMP, every host thread) stands in,
-on row samples of the same workload.
+reference is a Python/Numba package without a CPU path of its own for this
+kernel, so its CPU restatement (oracle/, C + OpenMP, every host thread)
+stands in, on row samples of the same workload.  The reference's own Numba
+CUDA kernel (installed under baseline/_ref) is timed beside ours on the
+1024 x 1024 workload (other_workloads.uniform_1k.reference_numba_kernel).
+
+--only NAME runs one of the other workloads alone (fingerprint, symmetric,
+uniform, overflow) and prints its result dict: the command profiler
+captures of those kernels use.
 """
 from __future__ import annotations
 
@@ -76,6 +82,11 @@ def parse():
     ap.add_argument("--config", type=str, default="", help="JSON cms_cosine_config override")
     ap.add_argument("--no-extra", action="store_true", help="skip the other workloads")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
+    ap.add_argument("--overflow-rows", type=int, default=1000,
+                    help="reference rows of the overflow-stress sample (20000: the whole matrix)")
+    ap.add_argument("--only", choices=["fingerprint", "symmetric", "uniform", "overflow"],
+                    default="", help="run only this one of the other workloads (for profiler "
+                                     "captures) and print its result instead of the bench line")
     return ap.parse_args()
 
 
@@ -213,6 +224,16 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def measured_bf16_tflops():
+    """Dense bf16 GEMM throughput (burst) from MEASURED_PEAKS.json, else the
+    pool's fallback figure."""
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["bf16_tflops"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 1590.0, "fallback"
+
+
 def sm_max_mhz(clock_summary=None):
     """Maximum SM clock: MEASURED_PEAKS.json's record when it has one, else the
     clocks.max.sm that nvidia-smi reported during the run."""
@@ -305,6 +326,10 @@ def run_ours(args, world, rank, local):
 
     dev = _native.require_cuda(local)
     torch.cuda.set_device(dev)
+    if args.only:  # one of the other workloads alone (profiler captures)
+        if rank == 0:
+            print(json.dumps(other_workloads(dev, args, only=args.only)), flush=True)
+        return
     ref, qry = make_data(args, rank)
     cfg = json.loads(args.config) if args.config else None
     tune_report = None
@@ -588,12 +613,23 @@ def _time_ms(fn, reps=3):
     return e0.elapsed_time(e1) / reps
 
 
-def other_workloads(dev, args):
-    """The other workloads, each bounded to seconds: device-resident pairs/s."""
+def other_workloads(dev, args, only=""):
+    """The other workloads, each bounded to seconds: device-resident pairs/s.
+    only: run just the named one ("fingerprint", "symmetric", "uniform",
+    "overflow")."""
+    res = {}
+    for name, fn in (("fingerprint", _fingerprint_workload), ("symmetric", _symmetric_workload),
+                     ("uniform", _uniform_workload), ("overflow", _overflow_workload)):
+        if only in ("", name):
+            res.update(fn(dev, args))
+    return res
+
+
+def _fingerprint_workload(dev, args):
     import numpy as np
     import torch
 
-    from cudams import autotune, kernels, synthetic
+    from cudams import kernels, synthetic
 
     res = {}
     # fingerprint similarity, 100k x 100k 2048-bit, jaccard/dice/cosine
@@ -628,18 +664,34 @@ def other_workloads(dev, args):
     tms = _time_ms(torch_jaccard)
     del R, Q
     torch.cuda.empty_cache()
-    mhz, _ = sm_max_mhz()
-    popc_peak = sm_count(dev) * 16 * mhz * 1e6 / 2  # popc64/s at 16 POPC32 per clock per SM
+    # tensor-core kernel: 2 int8 ops (multiply, add) per bit per pair; the
+    # int8 reference is twice the measured dense bf16 rate (the ratio of the
+    # nominal dense figures, 4.5 POPS : 2.25 PFLOP/s; no int8 GEMM is measured)
+    bf16, bf16_kind = measured_bf16_tflops()
+    ops_per_pair = 2 * 32 * bits.shape[1]
+    int8_peak = 2 * bf16 * 1e12
     res["fingerprint_100k"] = {
         "workload": f"{n_fp} x {n_fp} fingerprints, 2048 bits, density U(5%,15%)",
         "pairs_per_s": fp, "unit": "pairs/s",
-        "roofline": {"bound": "int-pipe popcount", "achieved_popc64_per_s": 32 * fp["jaccard"],
-                     "peak_popc64_per_s": popc_peak, "frac": 32 * fp["jaccard"] / popc_peak,
-                     "hbm_frac": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
+        "ms_per_measure": {m: n_fp * n_fp / v * 1e3 for m, v in fp.items()},
+        "roofline": {"bound": "tensor (int8)", "kernel": "fp_umma_kernel",
+                     "achieved_int8_ops_per_s": ops_per_pair * fp["jaccard"],
+                     "peak_int8_ops_per_s": int8_peak,
+                     "frac": ops_per_pair * fp["jaccard"] / int8_peak,
+                     "peak_source": f"2 x {bf16_kind} bf16_tflops (dense int8 : bf16 = 2 : 1)",
+                     "hbm_frac_output": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
         "reference_torch_cuda_jaccard_pairs_per_s": nt * nt / (tms / 1e3),
         "reference_torch_sample": f"{nt} x {nt}",
         "symmetric_jaccard_output_pairs_per_s": n_fp * n_fp / (ms_sym / 1e3)}
+    return res
 
+
+def _symmetric_workload(dev, args):
+    import torch
+
+    from cudams import autotune, kernels, synthetic
+
+    res = {}
     # is_symmetric=True greedy cosine on one set of the headline distribution:
     # upper triangle + mirror copy, against the full matrix of the same set
     n_sym = min(args.n, 40_000)
@@ -662,7 +714,15 @@ def other_workloads(dev, args):
     del sout, sd
     sset._device.clear()
     torch.cuda.empty_cache()
+    return res
 
+
+def _uniform_workload(dev, args):
+    import torch
+
+    from cudams import autotune, kernels, synthetic
+
+    res = {}
     # 1024 x 1024 uniform spectra, tol 0.1 (the reference's CPU-runnable case)
     u_r = synthetic.uniform_spectra(1024, seed=args.seed + 1).to_device(dev)
     u_q = synthetic.uniform_spectra(1024, seed=args.seed + 2).to_device(dev)
@@ -715,11 +775,20 @@ def other_workloads(dev, args):
                              "path": "CudaCosineGreedy.matrix(list of Spectrum objects) -> "
                                      "numpy structured array (packing + H2D + kernels + D2H)"}}
 
+    return res
+
+
+def _overflow_workload(dev, args):
+    import torch
+
+    from cudams import autotune, kernels, synthetic
+
+    res = {}
     # overflow stress: clustered dense spectra, 20k x 20k, nearly every pair overflows
     c_r = synthetic.clustered_spectra(20_000, seed=args.seed + 3)
     c_q = synthetic.clustered_spectra(20_000, seed=args.seed + 4)
     cfg = autotune.choose_config(c_r, c_q, 0.05)
-    rows = 1000
+    rows = max(1, min(c_r.n, args.overflow_rows))
     cr_sub = c_r.subset(0, rows).to_device(dev)
     cq = c_q.to_device(dev)
     cout = tuple(torch.empty((rows, c_q.n), dtype=t, device=dev)
