@@ -432,9 +432,9 @@ def run_ours(args, world, rank, local):
                        "tuning_measured": None if tune_report is None else {
                            "seconds": tune_report["seconds"],
                            "heuristic": tune_report["heuristic"],
-                           "tile_trials_ms": {str(t["tile_spectra"]): round(t["ms"], 4)
-                                              for t in tune_report["trials"]
-                                              if "tile_spectra" in t},
+                           "tile_trials_ns_per_pair": {
+                               str(t["tile_spectra"]): round(t["ns_per_pair"], 6)
+                               for t in tune_report["trials"] if "tile_spectra" in t},
                            "buckets": tune_report["buckets"]},
                        "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"row shards x{world}, no collective"},

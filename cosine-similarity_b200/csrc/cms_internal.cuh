@@ -18,6 +18,7 @@ enum : uint32_t {
     kErrSpectrumTooLong = 1u << 0,  // a spectrum exceeds CMS_MAX_PEAKS peaks
     kErrSpillOverrun = 1u << 1,     // sparse spill list capacity exceeded
     kErrBadOffsets = 1u << 2,       // offsets not non-decreasing / out of range
+    kErrPipelineTimeout = 1u << 3,  // a bounded hand-off wait between warps ran out
 };
 
 // One CSR spectrum set on the device (see the header comment of the public API).

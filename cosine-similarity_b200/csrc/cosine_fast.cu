@@ -354,6 +354,11 @@ struct JoinParams {
     int pool_max;            // candidates a sweep may hold: kPoolMax, or kPool without gpool
     int max_fetch;           // fetches of kFetch items per warp before it exits (0: no limit)
     unsigned char* gpool;    // global pool extension, kGPool * 16 bytes per warp (or null)
+    // bounded launches: a CTA claims one of n_slots global-pool slices (a bit
+    // of `slots`) for its lifetime instead of using slice blockIdx.x (null:
+    // slice blockIdx.x, persistent launches)
+    unsigned int* slots;
+    int n_slots;
     TraceOut trace;          // per-item timing records (rec null: off)
     unsigned long long* work;
     SpillList spill;
@@ -365,7 +370,8 @@ struct JoinParams {
 };
 
 constexpr int kFetch = 4;                  // work items taken per atomic
-constexpr int kSearchFetches = 4;          // fetches per warp of a library search's CTAs
+constexpr int kSearchWaves = 4;            // waves of short-lived CTAs per library search
+constexpr int kSlotWords = 64;             // slot bitmap words of a bounded join launch
 constexpr int kPoolMax = 4096;             // candidates per sweep: smem pool + global extension
 constexpr int kGPool = kPoolMax - kPool;   // global extension entries per warp
 static_assert(kPoolMax <= 4096, "pool slots are packed into 12 bits");
@@ -530,10 +536,43 @@ join_kernel(JoinParams P) {
     float* s_x = reinterpret_cast<float*>(slice + 16 * kPool + 4 * hw + 16 * 32 + 4 * kLongRuns);
     unsigned long long* s_t0 = reinterpret_cast<unsigned long long*>(
         slice + 16 * kPool + 4 * hw + 16 * 32 + 4 * kLongRuns + 4 * 32);
+    // Global-pool slice of this CTA: blockIdx.x, or under bounded launches a
+    // slice claimed from the slot bitmap (at most n_slots CTAs are resident at
+    // once, so one is free; if a release has not landed yet the CTA runs with
+    // the shared-memory pool only).  Every search is bounded by 2 passes over
+    // the words and 32 attempts per word.
+    __shared__ int s_slot;
+    int pslot = (int)blockIdx.x;
+    if (P.slots) {
+        if (threadIdx.x == 0) {
+            int got = -1;
+            const int words = (P.n_slots + 31) >> 5;
+            for (int i = 0; i < 2 * words && got < 0; ++i) {
+                const int w = (int)((blockIdx.x + (unsigned)i) % (unsigned)words);
+                const int nb = min(32, P.n_slots - 32 * w);
+                const unsigned valid = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
+                unsigned cur = atomicOr(&P.slots[w], 0u);
+                for (int k = 0; k < 32 && got < 0; ++k) {
+                    const unsigned freeb = ~cur & valid;
+                    if (!freeb) break;
+                    const unsigned bit = freeb & (0u - freeb);
+                    const unsigned old = atomicOr(&P.slots[w], bit);
+                    if (!(old & bit))
+                        got = 32 * w + (__ffs(bit) - 1);
+                    else
+                        cur = old | bit;
+                }
+            }
+            s_slot = got;
+        }
+        __syncthreads();
+        pslot = s_slot;
+    }
+    const int pool_max = (P.gpool && pslot >= 0) ? P.pool_max : kPool;
     Pool pool;
     {
-        const size_t gw = (size_t)blockIdx.x * kJoinWarps + (threadIdx.x >> 5);
-        unsigned char* g = P.gpool ? P.gpool + gw * (size_t)kGPool * 16 : nullptr;
+        const size_t gw = (size_t)(pslot >= 0 ? pslot : 0) * kJoinWarps + (threadIdx.x >> 5);
+        unsigned char* g = (P.gpool && pslot >= 0) ? P.gpool + gw * (size_t)kGPool * 16 : nullptr;
         pool.skey = reinterpret_cast<double*>(slice);
         pool.sgen = reinterpret_cast<uint32_t*>(slice + 8 * kPool);
         pool.smeta = reinterpret_cast<uint32_t*>(slice + 12 * kPool);
@@ -768,7 +807,7 @@ join_kernel(JoinParams P) {
                         const unsigned bal = __ballot_sync(full, cand);
                         const int slot = n + __popc(bal & below);
                         n += __popc(bal);
-                        if (cand && slot < P.pool_max) {
+                        if (cand && slot < pool_max) {
                             const int bq = (int)(en.id >> 16);
                             const int pB = (int)(en.id & 0xFFFFu);
                             const int pa = pc + o;
@@ -804,10 +843,10 @@ join_kernel(JoinParams P) {
                             pool.put(slot, key, gen, m);
                         }
                     }
-                    if (n > P.pool_max) break;
+                    if (n > pool_max) break;
                 }
                 __syncwarp();  // s_lh / s_wa / s_x are rewritten by the next step
-                if (n > P.pool_max) break;
+                if (n > pool_max) break;
                 if (pass == kPasses - 1) {  // next chunk: rotate the prefetched peaks
                     mz_c = mz_n;
                     w_c = w_n;
@@ -817,10 +856,10 @@ join_kernel(JoinParams P) {
                 }
             }
             __syncwarp();
-            if (n > P.pool_max) {
+            if (n > pool_max) {
                 if (rw > 1) {
                     // too many candidates for one pool: retry a narrower range
-                    width = max(1, (int)((long long)rw * P.pool_max / (2LL * n)));
+                    width = max(1, (int)((long long)rw * pool_max / (2LL * n)));
                     width = min(width, rw / 2 > 0 ? rw / 2 : 1);
                     continue;
                 }
@@ -1085,7 +1124,7 @@ join_kernel(JoinParams P) {
             flush_long();
             __syncwarp();
             range_lo = range_hi;
-            if (n < P.pool_max / 4) width = min(tn, width * 2);
+            if (n < pool_max / 4) width = min(tn, width * 2);
         }
         __syncwarp();
         if (P.trace.rec && lane == 0) {
@@ -1100,6 +1139,13 @@ join_kernel(JoinParams P) {
                 r[3] = global_ns();
             }
         }
+        }
+    }
+    if (P.slots) {  // give the global-pool slice back
+        __syncthreads();
+        if (threadIdx.x == 0 && pslot >= 0) {
+            atomicAnd(&P.slots[pslot >> 5], ~(1u << (pslot & 31)));
+            __threadfence();
         }
     }
 }
@@ -1159,8 +1205,23 @@ __device__ __forceinline__ void sort8_local(Cand (&c)[8], int base, int kk) {
         }
     }
 }
-__device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m) {
-    const int tid = threadIdx.x, nt = blockDim.x;
+// Barriers of the threads that generate and sort a pair's candidates: the
+// whole block, or (pipelined pair kernel) the producer warps only, on named
+// barrier 1.
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct GroupSync {
+    int n;  // participating threads (a multiple of 32)
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory");
+    }
+};
+
+// nt threads (tid 0..nt-1) sort okey/cgen[0, m), m = 8 * nt, in registers.
+template <typename Sync>
+__device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m, int nt, int tid,
+                            Sync sync) {
     const int base = 8 * tid;
     const unsigned full = 0xffffffffu;
     Cand c[8];
@@ -1177,13 +1238,13 @@ __device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m) {
                 const bool desc = (base & kk) == 0;  // kk >= 16: the same for all e
                 Cand o[8];
                 if (j >= 256) {
-                    __syncthreads();
+                    sync();
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         okey[e * nt + tid] = c[e].k;
                         cgen[e * nt + tid] = c[e].g;
                     }
-                    __syncthreads();
+                    sync();
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         o[e].k = okey[e * nt + pt];
@@ -1211,13 +1272,230 @@ __device__ void sort8_block(unsigned long long* okey, uint32_t* cgen, int m) {
             }
         }
     }
-    __syncthreads();
+    sync();
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         okey[base + e] = c[e].k;
         cgen[base + e] = c[e].g;
     }
-    __syncthreads();
+    sync();
+}
+
+// Candidates of pair (ri, qi) in generation order, truncated at match_limit,
+// into okey/cgen, by nt threads (tid 0..nt-1, whole warps) with barrier
+// `sync`; s_scan holds one int per warp.  Returns the number generated
+// before truncation stopped it (>= match_limit means overflow).
+template <bool MODIFIED, typename Sync>
+__device__ int gen_pair(const PairParams& P, int64_t ri, int64_t qi, unsigned long long* okey,
+                        uint32_t* cgen, int nt, int tid, int* s_scan, Sync sync) {
+    const int lane = tid & 31, wid = tid >> 5, nwarps = nt >> 5;
+    const unsigned full = 0xffffffffu;
+    const int64_t r0 = P.R.off[ri], q0 = P.Q.off[qi];
+    const int nr = (int)(P.R.off[ri + 1] - r0), nq = (int)(P.Q.off[qi + 1] - q0);
+    const float* qmz = P.Q.mz + q0;
+    int total = 0;
+    bool overflow = false;
+    // modified cosine generates twice: at shift 0, then at the pair's
+    // precursor difference, continuing the same candidate list
+#pragma unroll 1
+    for (int pass = 0; pass < (MODIFIED ? 2 : 1) && !overflow && nr > 0 && nq > 0; ++pass) {
+        const double shift = (MODIFIED && pass) ? __dsub_rn(P.R.prec[ri], P.Q.prec[qi]) : P.shift;
+        for (int pc = 0; pc < nr && !overflow; pc += nt) {
+            const int p1 = pc + tid;
+            int start = 0, cnt = 0;
+            double lo = 0.0, hi = 0.0, w1 = 0.0;
+            if (p1 < nr) {
+                const double mz1 = (double)P.R.mz[r0 + p1];
+                lo = __dsub_rn(mz1, P.tol);
+                hi = __dadd_rn(mz1, P.tol);
+                // first p2 with mz_q + shift >= lo
+                int L = 0, H = nq;
+                while (L < H) {
+                    const int M = (L + H) >> 1;
+                    if (__dadd_rn((double)qmz[M], shift) < lo)
+                        L = M + 1;
+                    else
+                        H = M;
+                }
+                start = L;
+                int k = L;
+                while (k < nq && !(__dadd_rn((double)qmz[k], shift) > hi)) ++k;
+                cnt = k - L;
+            }
+            // exclusive scan of cnt over the nt threads
+            int incl = cnt;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(full, incl, d);
+                if (lane >= d) incl += v;
+            }
+            if (lane == 31) s_scan[wid] = incl;
+            sync();
+            if (wid == 0) {
+                int v = lane < nwarps ? s_scan[lane] : 0;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int u = __shfl_up_sync(full, v, d);
+                    if (lane >= d) v += u;
+                }
+                if (lane < nwarps) s_scan[lane] = v;
+            }
+            sync();
+            const int excl = incl - cnt + (wid > 0 ? s_scan[wid - 1] : 0);
+            const int chunk_total = s_scan[nwarps - 1];
+            if (cnt > 0) {
+                w1 = __dmul_rn(peak_a(P.R.a, r0 + p1), P.R.b[r0 + p1]);
+                for (int i = 0; i < cnt; ++i) {
+                    const int rank = total + excl + i;
+                    if (rank >= P.match_limit) break;
+                    const int p2 = start + i;
+                    const double key =
+                        __dmul_rn(__dmul_rn(w1, peak_a(P.Q.a, q0 + p2)), P.Q.b[q0 + p2]);
+                    okey[rank] = order_key(key);
+                    cgen[rank] = ((uint32_t)pass << 31) | ((uint32_t)p1 << 16) | (uint32_t)p2;
+                }
+            }
+            total += chunk_total;
+            if (total >= P.match_limit) overflow = true;
+            sync();
+        }
+    }
+    return total;
+}
+
+// Pads okey/cgen[n, m) and sorts [0, m) descending by (okey, gen), m the
+// power of two >= n: in registers when m = 8 * nt, else in shared memory.
+template <typename Sync>
+__device__ void sort_pair(unsigned long long* okey, uint32_t* cgen, int n, int m, int nt, int tid,
+                          Sync sync) {
+    for (int i = n + tid; i < m; i += nt) {
+        okey[i] = 0ull;
+        cgen[i] = 0u;
+    }
+    sync();
+    if (m == 8 * nt) {
+        sort8_block(okey, cgen, m, nt, tid, sync);
+        return;
+    }
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < m; i += nt) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long ka = okey[i], kb = okey[ixj];
+                    const uint32_t ga = cgen[i], gb = cgen[ixj];
+                    const bool a_gt_b = ka > kb || (ka == kb && ga > gb);
+                    const bool desc = (i & k) == 0;
+                    if (desc ? !a_gt_b : a_gt_b) {
+                        okey[i] = kb;
+                        okey[ixj] = ka;
+                        cgen[i] = gb;
+                        cgen[ixj] = ga;
+                    }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+// Greedy by one warp over chunks of 32 sorted candidates (used_r / used_q
+// zeroed for the pair's peaks).  Within a chunk a live candidate is accepted
+// iff no earlier accepted one shares its reference or query peak: conflict
+// masks come from __match_any_sync, and lanes decide in rounds, each lane as
+// soon as every earlier conflicting lane has decided (the lowest undecided
+// lane always can, so this ends; usually after one or two rounds).  Accepted
+// keys are summed in sorted order, as the sequential greedy; every lane ends
+// with the same score and match count.
+template <bool MODIFIED>
+__device__ void greedy_pair(const unsigned long long* okey, const uint32_t* cgen,
+                            uint32_t* used_r, uint32_t* used_q, int n, double& score,
+                            int& matches) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    // the next chunk's candidates are loaded while this one is resolved
+    // (they do not depend on the used-peak bits)
+    uint32_t g_nx = lane < n ? cgen[lane] : 0u;
+    unsigned long long k_nx = lane < n ? okey[lane] : 0ull;
+    for (int c = 0; c < n; c += 32) {
+        const int i = c + lane;
+        const uint32_t g = g_nx;
+        const unsigned long long ok = k_nx;
+        if (i + 32 < n) {
+            g_nx = cgen[i + 32];
+            k_nx = okey[i + 32];
+        }
+        bool alive = false;
+        if (i < n) {
+            const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
+            alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
+                    !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
+        }
+        const unsigned live = __ballot_sync(full, alive);
+        if (live == 0u) continue;
+        // dead lanes get values no peak index takes, so they match only
+        // themselves
+        const unsigned m1 = __match_any_sync(full, alive ? gen_p1<MODIFIED>(g) : 0x10000u + lane);
+        const unsigned m2 = __match_any_sync(full, alive ? (g & 0xFFFFu) : 0x10000u + lane);
+        const unsigned earlier = (m1 | m2) & live & below;
+        unsigned dec = ~live, acc = 0u;
+        while (dec != full) {
+            bool my_dec = (dec >> lane) & 1u, my_acc = (acc >> lane) & 1u;
+            if (!my_dec && (earlier & ~dec) == 0u) {
+                my_dec = true;
+                my_acc = (earlier & acc) == 0u;
+            }
+            dec = __ballot_sync(full, my_dec);
+            acc = __ballot_sync(full, my_acc);
+        }
+        if ((acc >> lane) & 1u) {
+            const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
+            atomicOr(&used_r[p1 >> 5], 1u << (p1 & 31));
+            atomicOr(&used_q[p2 >> 5], 1u << (p2 & 31));
+        }
+        const double kk = (i < n) ? key_from_order(ok) : 0.0;
+        for (unsigned a = acc; a; a &= a - 1u) {
+            const double k = __shfl_sync(full, kk, __ffs(a) - 1);
+            score = __dadd_rn(score, k);
+        }
+        matches += __popc(acc);
+        __syncwarp();
+    }
+}
+
+// The pair's outputs (dense, or a sparse hit above the threshold).
+template <bool SPARSE>
+__device__ void write_pair(const PairParams& P, int64_t ri, int64_t qi, int n, double score,
+                           int matches, bool overflow) {
+    float sc = 0.f;
+    if (matches > 0 || n > 0) {
+        const double denom = __dmul_rn(P.snR[ri], P.snQ[qi]);
+        sc = (n > 0) ? (float)__ddiv_rn(score, denom) : 0.f;
+    }
+    if (!SPARSE) {
+        const int64_t o = ri * P.dense.ld + qi;
+        P.dense.score[o] = sc;
+        P.dense.matches[o] = matches;
+        P.dense.overflow[o] = overflow ? 1 : 0;
+    } else if (n > 0 && sc >= P.sparse.threshold) {
+        emit_hit(P.sparse, (int)ri, (int)qi, sc, matches, overflow ? 1 : 0);
+    }
+}
+
+// item -> pair (reference ri, query qi); false for pairs under the diagonal
+// of a symmetric whole-matrix launch (copied afterwards)
+__device__ __forceinline__ bool pair_of(const PairParams& P, int64_t item, int64_t& ri,
+                                        int64_t& qi) {
+    if (P.pairs) {
+        const int2 pr = P.pairs[item];
+        ri = pr.x;
+        qi = pr.y;
+        return true;
+    }
+    ri = item / P.Q.n;
+    qi = item - ri * P.Q.n;
+    return !(P.sym && ri > qi);
 }
 
 template <bool SPARSE, bool MODIFIED>
@@ -1231,10 +1509,9 @@ __global__ void pair_kernel(PairParams P) {
     __shared__ int s_scan[32];
     __shared__ unsigned long long s_item;
 
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int nwarps = blockDim.x >> 5;
-    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, wid = tid >> 5;
     const int64_t n_items = P.pairs ? (int64_t)min(*P.n_pairs, P.pairs_cap) : P.R.n * P.Q.n;
+    const BlockSync sync;
 
     for (int64_t iter = 0;; ++iter) {
         // spill list: dynamic (pairs differ widely in cost); whole matrix:
@@ -1246,199 +1523,195 @@ __global__ void pair_kernel(PairParams P) {
         const int64_t item = (int64_t)s_item;
         if (item >= n_items) break;
         int64_t ri, qi;
-        if (P.pairs) {
-            const int2 pr = P.pairs[item];
-            ri = pr.x;
-            qi = pr.y;
-        } else {
-            ri = item / P.Q.n;
-            qi = item - ri * P.Q.n;
-            if (P.sym && ri > qi) continue;  // the lower triangle is copied afterwards
-        }
-        const int64_t r0 = P.R.off[ri], q0 = P.Q.off[qi];
-        const int nr = (int)(P.R.off[ri + 1] - r0), nq = (int)(P.Q.off[qi + 1] - q0);
-        const float* qmz = P.Q.mz + q0;
-
-        int total = 0;
-        bool overflow = false;
-        // modified cosine generates twice: at shift 0, then at the pair's
-        // precursor difference, continuing the same candidate list
-#pragma unroll 1
-        for (int pass = 0; pass < (MODIFIED ? 2 : 1) && !overflow && nr > 0 && nq > 0; ++pass) {
-            const double shift =
-                (MODIFIED && pass) ? __dsub_rn(P.R.prec[ri], P.Q.prec[qi]) : P.shift;
-            for (int pc = 0; pc < nr && !overflow; pc += blockDim.x) {
-                const int p1 = pc + tid;
-                int start = 0, cnt = 0;
-                double lo = 0.0, hi = 0.0, w1 = 0.0;
-                if (p1 < nr) {
-                    const double mz1 = (double)P.R.mz[r0 + p1];
-                    lo = __dsub_rn(mz1, P.tol);
-                    hi = __dadd_rn(mz1, P.tol);
-                    // first p2 with mz_q + shift >= lo
-                    int L = 0, H = nq;
-                    while (L < H) {
-                        const int M = (L + H) >> 1;
-                        if (__dadd_rn((double)qmz[M], shift) < lo)
-                            L = M + 1;
-                        else
-                            H = M;
-                    }
-                    start = L;
-                    int k = L;
-                    while (k < nq && !(__dadd_rn((double)qmz[k], shift) > hi)) ++k;
-                    cnt = k - L;
-                }
-                // block exclusive scan of cnt
-                int incl = cnt;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const int v = __shfl_up_sync(full, incl, d);
-                    if (lane >= d) incl += v;
-                }
-                if (lane == 31) s_scan[wid] = incl;
-                __syncthreads();
-                if (wid == 0) {
-                    int v = lane < nwarps ? s_scan[lane] : 0;
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const int u = __shfl_up_sync(full, v, d);
-                        if (lane >= d) v += u;
-                    }
-                    if (lane < nwarps) s_scan[lane] = v;
-                }
-                __syncthreads();
-                const int excl = incl - cnt + (wid > 0 ? s_scan[wid - 1] : 0);
-                const int chunk_total = s_scan[nwarps - 1];
-                if (cnt > 0) {
-                    w1 = __dmul_rn(peak_a(P.R.a, r0 + p1), P.R.b[r0 + p1]);
-                    for (int i = 0; i < cnt; ++i) {
-                        const int rank = total + excl + i;
-                        if (rank >= P.match_limit) break;
-                        const int p2 = start + i;
-                        const double key =
-                            __dmul_rn(__dmul_rn(w1, peak_a(P.Q.a, q0 + p2)), P.Q.b[q0 + p2]);
-                        okey[rank] = order_key(key);
-                        cgen[rank] = ((uint32_t)pass << 31) | ((uint32_t)p1 << 16) | (uint32_t)p2;
-                    }
-                }
-                total += chunk_total;
-                if (total >= P.match_limit) overflow = true;
-                __syncthreads();
-            }
-        }
+        if (!pair_of(P, item, ri, qi)) continue;
+        const int total = gen_pair<MODIFIED>(P, ri, qi, okey, cgen, blockDim.x, tid, s_scan, sync);
         const int n = min(total, P.match_limit);
         double score = 0.0;
         int matches = 0;
         if (n > 0) {
-            int m = 1;
-            while (m < n) m <<= 1;
-            for (int i = n + tid; i < m; i += blockDim.x) {
-                okey[i] = 0ull;
-                cgen[i] = 0u;
-            }
+            const int nr = (int)(P.R.off[ri + 1] - P.R.off[ri]);
+            const int nq = (int)(P.Q.off[qi + 1] - P.Q.off[qi]);
             for (int i = tid; i < (nr + 31) / 32; i += blockDim.x) used_r[i] = 0u;
             for (int i = tid; i < (nq + 31) / 32; i += blockDim.x) used_q[i] = 0u;
-            __syncthreads();
-            // bitonic sort, descending by (okey, gen): in registers when the
-            // block holds exactly eight candidates a thread, else in shared memory
-            if (m == 8 * (int)blockDim.x) {
-                sort8_block(okey, cgen, m);
-            } else
-            for (int k = 2; k <= m; k <<= 1) {
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    for (int i = tid; i < m; i += blockDim.x) {
-                        const int ixj = i ^ j;
-                        if (ixj > i) {
-                            const unsigned long long ka = okey[i], kb = okey[ixj];
-                            const uint32_t ga = cgen[i], gb = cgen[ixj];
-                            const bool a_gt_b = ka > kb || (ka == kb && ga > gb);
-                            const bool desc = (i & k) == 0;
-                            if (desc ? !a_gt_b : a_gt_b) {
-                                okey[i] = kb;
-                                okey[ixj] = ka;
-                                cgen[i] = gb;
-                                cgen[ixj] = ga;
-                            }
-                        }
-                    }
-                    __syncthreads();
+            int m = 1;
+            while (m < n) m <<= 1;
+            sort_pair(okey, cgen, n, m, blockDim.x, tid, sync);
+            if (wid == 0) greedy_pair<MODIFIED>(okey, cgen, used_r, used_q, n, score, matches);
+        }
+        if (tid == 0) write_pair<SPARSE>(P, ri, qi, n, score, matches, total >= P.match_limit);
+    }
+}
+
+// ---- pipelined pair kernel ----
+// Warps 0..G-1 (the producers, G = blockDim.x / 32 - 1) generate and sort the
+// candidates of the next pair into one of two buffers while warp G (the
+// consumer) runs the greedy of the previous pair from the other buffer, so the
+// producers never wait at a barrier while one warp resolves.  The hand-off
+// is two mbarriers per buffer: `full` (every producer thread arrives after
+// its writes) and `empty` (the consumer, after reading).  Every wait is
+// bounded by %globaltimer (kPipeWaitNs); on expiry the waiting side sets
+// kErrPipelineTimeout, raises the CTA's stop flag and leaves, and the other
+// side leaves at its next (bounded) wait.  The producers of a CTA take every
+// decision together (one thread decides, a producer barrier publishes it),
+// so their named barrier is never left half-joined.
+constexpr unsigned long long kPipeWaitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long pipe_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void pipe_bar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(bar)),
+                 "r"(count));
+}
+__device__ __forceinline__ void pipe_bar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(bar))
+                 : "memory");
+}
+// true once the phase of `parity` has completed; false after kPipeWaitNs or
+// when *stop is raised
+__device__ __forceinline__ bool pipe_bar_wait(uint64_t* bar, uint32_t parity,
+                                              volatile int* stop) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    const unsigned long long t0 = pipe_clock();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (*stop) return false;
+        if (pipe_clock() - t0 > kPipeWaitNs) return false;
+    }
+}
+
+template <bool SPARSE, bool MODIFIED>
+__global__ void pair_kernel_pipe(PairParams P) {
+    if (*P.bad) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // two candidate buffers, then the consumer's used-peak bitmaps
+    unsigned long long* okey0 = reinterpret_cast<unsigned long long*>(smem_raw);
+    uint32_t* cgen0 = reinterpret_cast<uint32_t*>(okey0 + 2 * P.cap);
+    uint32_t* used_r = cgen0 + 2 * P.cap;  // 2048 words: 65536 peaks
+    uint32_t* used_q = used_r + 2048;
+    __shared__ int s_scan[32];
+    __shared__ unsigned long long s_item;
+    __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+    __shared__ long long s_ri[2], s_qi[2];
+    __shared__ int s_total[2];  // candidates generated; -1: no more pairs
+    __shared__ int s_go;        // producers: 1 to continue
+    __shared__ volatile int s_stop;
+
+    const int tid = threadIdx.x;
+    const int np = (int)blockDim.x - 32;  // producer threads
+    const bool producer = tid < np;
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            pipe_bar_init(&s_full[b], (uint32_t)np);
+            pipe_bar_init(&s_empty[b], 1u);
+        }
+        s_stop = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int64_t n_items = P.pairs ? (int64_t)min(*P.n_pairs, P.pairs_cap) : P.R.n * P.Q.n;
+
+    if (producer) {
+        const GroupSync sync{np};
+        int b = 0;
+        uint32_t ph = 0;  // parity of buffer b's current use
+        for (int64_t iter = 0;; ++iter) {
+            if (tid == 0) s_item = P.pairs ? atomicAdd(P.work, 1ull)
+                                           : (unsigned long long)(blockIdx.x + iter * gridDim.x);
+            sync();
+            const int64_t item = (int64_t)s_item;
+            int64_t ri = 0, qi = 0;
+            const bool more = item < n_items;
+            if (more && !pair_of(P, item, ri, qi)) {
+                sync();  // s_item is rewritten by the next fetch
+                continue;
+            }
+            // buffer b free (the consumer is done with its previous pair)?
+            if (tid == 0) s_go = pipe_bar_wait(&s_empty[b], ph ^ 1u, &s_stop) ? 1 : 0;
+            sync();
+            if (!s_go) {
+                if (tid == 0 && !s_stop) {
+                    atomicOr(P.err, kErrPipelineTimeout);
+                    s_stop = 1;
+                }
+                break;
+            }
+            unsigned long long* okey = okey0 + (size_t)b * P.cap;
+            uint32_t* cgen = cgen0 + (size_t)b * P.cap;
+            int total = -1;
+            if (more) {
+                total = gen_pair<MODIFIED>(P, ri, qi, okey, cgen, np, tid, s_scan, sync);
+                const int n = min(total, P.match_limit);
+                if (n > 0) {
+                    int m = 1;
+                    while (m < n) m <<= 1;
+                    sort_pair(okey, cgen, n, m, np, tid, sync);
                 }
             }
-            // greedy by warp 0 over chunks of 32 sorted candidates.  Within a
-            // chunk a live candidate is accepted iff no earlier accepted one
-            // shares its reference or query peak: conflict masks come from
-            // __match_any_sync, and lanes decide in rounds, each lane as soon as
-            // every earlier conflicting lane has decided (the lowest undecided
-            // lane always can, so this ends; usually after one or two rounds).
-            // Accepted keys are summed in sorted order, as the sequential greedy.
-            if (wid == 0) {
-                const unsigned below = (1u << lane) - 1u;
-                // the next chunk's candidates are loaded while this one is
-                // resolved (they do not depend on the used-peak bits)
-                uint32_t g_nx = lane < n ? cgen[lane] : 0u;
-                unsigned long long k_nx = lane < n ? okey[lane] : 0ull;
-                for (int c = 0; c < n; c += 32) {
-                    const int i = c + lane;
-                    const uint32_t g = g_nx;
-                    const unsigned long long ok = k_nx;
-                    if (i + 32 < n) {
-                        g_nx = cgen[i + 32];
-                        k_nx = okey[i + 32];
-                    }
-                    bool alive = false;
-                    if (i < n) {
-                        const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
-                        alive = !((used_r[p1 >> 5] >> (p1 & 31)) & 1u) &&
-                                !((used_q[p2 >> 5] >> (p2 & 31)) & 1u);
-                    }
-                    const unsigned live = __ballot_sync(full, alive);
-                    if (live == 0u) continue;
-                    // dead lanes get values no peak index takes, so they match
-                    // only themselves
-                    const unsigned m1 =
-                        __match_any_sync(full, alive ? gen_p1<MODIFIED>(g) : 0x10000u + lane);
-                    const unsigned m2 =
-                        __match_any_sync(full, alive ? (g & 0xFFFFu) : 0x10000u + lane);
-                    const unsigned earlier = (m1 | m2) & live & below;
-                    unsigned dec = ~live, acc = 0u;
-                    while (dec != full) {
-                        bool my_dec = (dec >> lane) & 1u, my_acc = (acc >> lane) & 1u;
-                        if (!my_dec && (earlier & ~dec) == 0u) {
-                            my_dec = true;
-                            my_acc = (earlier & acc) == 0u;
-                        }
-                        dec = __ballot_sync(full, my_dec);
-                        acc = __ballot_sync(full, my_acc);
-                    }
-                    if ((acc >> lane) & 1u) {
-                        const int p1 = (int)gen_p1<MODIFIED>(g), p2 = g & 0xFFFF;
-                        atomicOr(&used_r[p1 >> 5], 1u << (p1 & 31));
-                        atomicOr(&used_q[p2 >> 5], 1u << (p2 & 31));
-                    }
-                    const double kk = (i < n) ? key_from_order(ok) : 0.0;
-                    for (unsigned a = acc; a; a &= a - 1u) {
-                        const double k = __shfl_sync(full, kk, __ffs(a) - 1);
-                        score = __dadd_rn(score, k);
-                    }
-                    matches += __popc(acc);
-                    __syncwarp();
-                }
+            if (tid == 0) {
+                s_ri[b] = ri;
+                s_qi[b] = qi;
+                s_total[b] = total;
+            }
+            sync();
+            pipe_bar_arrive(&s_full[b]);
+            if (!more) break;
+            if (++b == 2) {
+                b = 0;
+                ph ^= 1u;
             }
         }
-        if (tid == 0) {
-            float sc = 0.f;
-            if (matches > 0 || n > 0) {
-                const double denom = __dmul_rn(P.snR[ri], P.snQ[qi]);
-                sc = (n > 0) ? (float)__ddiv_rn(score, denom) : 0.f;
+    } else {
+        // consumer warp
+        const int lane = tid & 31;
+        int b = 0;
+        uint32_t ph = 0;
+        for (;;) {
+            int ok = 0;
+            if (lane == 0) ok = pipe_bar_wait(&s_full[b], ph, &s_stop) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0 && !s_stop) {
+                    atomicOr(P.err, kErrPipelineTimeout);
+                    s_stop = 1;
+                }
+                break;
             }
-            if (!SPARSE) {
-                const int64_t o = ri * P.dense.ld + qi;
-                P.dense.score[o] = sc;
-                P.dense.matches[o] = matches;
-                P.dense.overflow[o] = overflow ? 1 : 0;
-            } else if (n > 0 && sc >= P.sparse.threshold) {
-                emit_hit(P.sparse, (int)ri, (int)qi, sc, matches, overflow ? 1 : 0);
+            const int total = s_total[b];
+            if (total < 0) break;  // no more pairs
+            const int64_t ri = s_ri[b], qi = s_qi[b];
+            const int n = min(total, P.match_limit);
+            double score = 0.0;
+            int matches = 0;
+            if (n > 0) {
+                const int nr = (int)(P.R.off[ri + 1] - P.R.off[ri]);
+                const int nq = (int)(P.Q.off[qi + 1] - P.Q.off[qi]);
+                for (int i = lane; i < (nr + 31) / 32; i += 32) used_r[i] = 0u;
+                for (int i = lane; i < (nq + 31) / 32; i += 32) used_q[i] = 0u;
+                __syncwarp();
+                greedy_pair<MODIFIED>(okey0 + (size_t)b * P.cap, cgen0 + (size_t)b * P.cap,
+                                      used_r, used_q, n, score, matches);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                pipe_bar_arrive(&s_empty[b]);
+                write_pair<SPARSE>(P, ri, qi, n, score, matches, total >= P.match_limit);
+            }
+            if (++b == 2) {
+                b = 0;
+                ph ^= 1u;
             }
         }
     }
@@ -1535,31 +1808,43 @@ int set_func_smem(T* f, size_t bytes) {
     return raise_func_smem(reinterpret_cast<const void*>(f), bytes);
 }
 
-// Launch the join.  Persistent (jp.max_fetch == 0): one resident CTA per
-// slot, each warp pulling work until none is left; its warps own the global
-// pool slices, so the grid may not exceed the resident CTAs.  Bounded
-// (jp.max_fetch > 0, no global pool): enough short-lived CTAs for the work,
-// each warp exiting after max_fetch fetches, so that the SMs free up CTA by
-// CTA and concurrent launches on other streams are scheduled in between.
+// Launch the join.  Persistent (waves == 0): one resident CTA per slot, each
+// warp pulling work until none is left; CTA b owns global-pool slices
+// 8b..8b+7, so the grid may not exceed the resident CTAs.  Bounded
+// (waves > 0): `waves` times the resident CTAs, each warp exiting after an
+// equal share of fetches, so that the SMs free up CTA by CTA and concurrent
+// launches on other streams are scheduled in between while every wave stays
+// full; each CTA claims a global-pool slice from jp.slots (zeroed by the
+// caller) for its lifetime.
 template <bool A_IS_REF, bool SPARSE, bool NOSHIFT, bool MODIFIED>
 int launch_join(cms_ctx* ctx, JoinParams jp, size_t smem, size_t gpool_warps, int64_t n_items,
-                cudaStream_t s) {
+                cudaStream_t s, int waves = 0) {
     auto* kern = join_kernel<A_IS_REF, SPARSE, NOSHIFT, MODIFIED>;
     if (const int rc = set_func_smem(kern, smem)) return rc;
     jp.trace = TraceOut{ctx->trace_rec, ctx->trace_count, ctx->trace_cap, ctx->trace_tag};
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
+    const int64_t resident = (int64_t)ctx->sm_count * std::max(1, per_sm);
     int64_t grid;
-    if (jp.max_fetch > 0) {
-        const int64_t per_cta = (int64_t)kJoinWarps * kFetch * jp.max_fetch;
-        grid = std::max<int64_t>(1, (n_items + per_cta - 1) / per_cta);
-        if (grid > INT32_MAX) {
+    if (waves > 0) {
+        const int64_t fetches = std::max<int64_t>(1, (n_items + kFetch - 1) / kFetch);
+        grid = std::min<int64_t>(resident * waves, (fetches + kJoinWarps - 1) / kJoinWarps);
+        grid = std::max<int64_t>(1, grid);
+        const int64_t per_warp = (fetches + grid * kJoinWarps - 1) / (grid * kJoinWarps);
+        if (per_warp > INT32_MAX) {
             set_error("cms_cosine_greedy: too many work items for one launch");
             return CMS_ERR_UNSUPPORTED;
         }
+        jp.max_fetch = (int)per_warp;
+        if (!jp.slots) jp.gpool = nullptr;
+        jp.n_slots = (int)std::min<int64_t>(resident, (int64_t)(gpool_warps / kJoinWarps));
+        if (jp.n_slots <= 0) jp.gpool = nullptr;
+        if (!jp.gpool) jp.pool_max = kPool;
     } else {
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kJoinThreads, smem);
-        grid = (int64_t)ctx->sm_count * std::max(1, per_sm);
-        if ((size_t)grid * kJoinWarps > gpool_warps) {
+        jp.max_fetch = 0;
+        jp.slots = nullptr;
+        grid = resident;
+        if (jp.gpool && (size_t)grid * kJoinWarps > gpool_warps) {
             set_error("cms_cosine_greedy: join grid larger than its scratch");
             return CMS_ERR_CUDA;
         }
@@ -1700,7 +1985,24 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     pair_blocks_per_sm = std::max(1, pair_blocks_per_sm);
     const int pair_grid = ctx->sm_count * pair_blocks_per_sm;
 
-    if (p.mode == 2) {
+    if (p.mode == 2 && pair_smem + (size_t)p.cap * 12 <= ctx->smem_optin) {
+        // whole matrix: the pipelined pair kernel (pair_threads producers
+        // plus a consumer warp, two candidate buffers)
+        void (*pipe_k)(PairParams) =
+            sparse ? (args.modified ? pair_kernel_pipe<true, true> : pair_kernel_pipe<true, false>)
+                   : (args.modified ? pair_kernel_pipe<false, true>
+                                    : pair_kernel_pipe<false, false>);
+        const size_t pipe_smem = pair_smem + (size_t)p.cap * 12;
+        const int pipe_threads = p.pair_threads + 32;
+        if ((rc = set_func_smem(pipe_k, pipe_smem))) return rc;
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipe_k, pipe_threads, pipe_smem);
+        StageScope sc(ctx, 4, 1, s);
+        pipe_k<<<ctx->sm_count * std::max(1, per_sm), pipe_threads, pipe_smem, s>>>(pp);
+        CMS_CUDA_TRY(cudaGetLastError());
+        return mirror();
+    }
+    if (p.mode == 2) {  // one candidate buffer only fits
         StageScope sc(ctx, 4, 1, s);
         pair_k<<<pair_grid, p.pair_threads, pair_smem, s>>>(pp);
         CMS_CUDA_TRY(cudaGetLastError());
@@ -2413,9 +2715,14 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     const long long items = (long long)n_q * lib->g.n_tiles;
     const unsigned int spill_cap =
         (unsigned int)std::min<long long>(std::max<long long>(1 << 16, items), 1 << 24);
+    // global-pool slices for up to four resident CTAs per SM (more CTAs per
+    // SM run with the shared-memory pool only)
+    const size_t gpool_warps =
+        (size_t)std::min(ctx->sm_count * 4, kSlotWords * 32) * kJoinWarps;
+    const size_t gpool_bytes = gpool_warps * (size_t)kGPool * 16;
     size_t need = bump_size(64 * sizeof(uint64_t)) + bump_size(n_q * sizeof(double)) +
                   bump_size(n_q * sizeof(int32_t)) + bump_size((size_t)spill_cap * sizeof(int2)) +
-                  4096;
+                  bump_size(kSlotWords * sizeof(uint32_t)) + bump_size(gpool_bytes) + 4096;
     int rc = arena_reserve(ctx, ctx->scratch, need, s);
     if (rc) return rc;
     Bump bp{(char*)ctx->scratch.ptr, 0, ctx->scratch.bytes};
@@ -2429,7 +2736,10 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     double* snQ = bp.take<double>(n_q);
     int32_t* order = bp.take<int32_t>(n_q);
     int2* spill = bp.take<int2>(spill_cap);
+    uint32_t* slots = bp.take<uint32_t>(kSlotWords);
+    unsigned char* gpool = bp.take<unsigned char>(gpool_bytes);
     CMS_CUDA_TRY(cudaMemsetAsync(small, 0, 64 * sizeof(uint64_t), s));
+    CMS_CUDA_TRY(cudaMemsetAsync(slots, 0, kSlotWords * sizeof(uint32_t), s));
 
     const int threads = 256;
     auto grid_for = [&](int64_t cnt) {
@@ -2463,11 +2773,12 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     jp.tol = lib->tol;
     jp.shift = lib->shift;
     jp.match_limit = lib->match_limit;
-    // A search runs as short-lived CTAs (bounded fetches per warp) so that
-    // searches on other streams interleave with it on the device; without
-    // resident warps there is no global pool, only the shared-memory one.
-    jp.pool_max = kPool;
-    jp.max_fetch = kSearchFetches;
+    // A search runs as kSearchWaves waves of short-lived CTAs (an equal share
+    // of fetches per warp) so that searches on other streams interleave with
+    // it on the device; each CTA claims a global-pool slice while it lives.
+    jp.pool_max = kPoolMax;
+    jp.gpool = gpool;
+    jp.slots = slots;
     jp.init_width_scale = 0.f;
     if (lib->cand_per_pair > 0.0 && n_q > 0) {
         const double mean_na = (double)n_q_peaks / (double)n_q;
@@ -2475,7 +2786,6 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
         jp.init_width_scale = (float)(0.5 * jp.pool_max / lambda);
     }
     jp.warp_smem_bytes = warp_slice_bytes(lib->g.tile);
-    jp.gpool = nullptr;
     jp.work = work_join;
     jp.spill = SpillList{spill, spill_count, spill_cap};
     jp.dense = DenseOut{nullptr, nullptr, nullptr, 0};
@@ -2485,8 +2795,8 @@ extern "C" int cms_library_search(cms_ctx* ctx, const cms_library* lib, const fl
     {
         StageScope sc(ctx, 3, 1, s);
         rc = launch_join<false, true, false, false>(ctx, jp,
-                                                    (size_t)jp.warp_smem_bytes * kJoinWarps, 0,
-                                                    items, s);
+                                                    (size_t)jp.warp_smem_bytes * kJoinWarps,
+                                                    gpool_warps, items, s, kSearchWaves);
         if (rc) return rc;
     }
     PairParams pp{};

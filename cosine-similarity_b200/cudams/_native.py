@@ -25,6 +25,7 @@ CMS_ERR_DEVICE = 6
 DEVERR_SPECTRUM_TOO_LONG = 1
 DEVERR_SPILL_OVERRUN = 2
 DEVERR_BAD_OFFSETS = 4
+DEVERR_PIPELINE_TIMEOUT = 8
 
 FP_MEASURES = {"jaccard": 0, "dice": 1, "cosine": 2}
 
@@ -240,12 +241,15 @@ def stream_handle(stream) -> c_void_p:
 
 
 def require_cuda(device=None):
-    """Return a torch.device on a B200, or raise (no CPU fallback)."""
+    """Return a torch.device on a B200, or raise (no CPU fallback).  device:
+    None (the current device), an index, or a torch.device."""
     import torch
 
     if not torch.cuda.is_available():
         raise NativeError("no CUDA device is available; cudams has no CPU fallback",
                           CMS_ERR_UNSUPPORTED)
+    if isinstance(device, torch.device):
+        device = device.index
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
     major, _ = torch.cuda.get_device_capability(dev)
     if major != 10:

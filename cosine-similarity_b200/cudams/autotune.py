@@ -176,12 +176,18 @@ class Tuner:
 
     def measure(self, ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
                 shift: float = 0.0, match_limit: int = 2048, device=None, gpu: str = "B200",
-                sample_ref: int = 4096, sample_qry: int = 20000, reps: int = 3,
-                record: bool = True, seed: int = 0):
+                sample_ref: int = 100000, tiles_per_trial: int = 3, class_sample: int = 1024,
+                reps: int = 3, record: bool = True, seed: int = 0):
         """Choose tile_spectra and width_by_class by timed trials on the device.
 
-        Returns (config, report); report lists every trial (ms per trial on
-        the sample) and the chosen setting per bucket."""
+        Tile trials sweep (a sample of at most sample_ref of) the reference
+        spectra over the first tiles_per_trial tiles of queries, so that every
+        tile is swept by as many references as at full size (how often a tile
+        stream is reused decides how much its first load from DRAM costs);
+        tiles are ranked by time per pair.  Width trials then time, per length
+        class of the references, up to class_sample spectra of that class over
+        the same query tiles.  Returns (config, report); report lists every
+        trial (ms on its sample) and the chosen setting per bucket."""
         import time
 
         import torch
@@ -197,19 +203,23 @@ class Tuner:
             report["seconds"] = time.perf_counter() - t_start
             return base, report
         rng = np.random.default_rng(seed)
-        qs = qry.subset(0, min(qry.n, sample_qry))
-        qd = qs.to_device(dev)
         lengths = ref.lengths
         classes = np.where(lengths > 0, np.floor(np.log2(np.maximum(lengths, 1))).astype(int) + 1, 0)
-        pick = np.sort(rng.choice(ref.n, min(ref.n, sample_ref), replace=False))
-        rs = ref.take(pick)
+        if ref.n > sample_ref:
+            rs = ref.take(np.sort(rng.choice(ref.n, sample_ref, replace=False)))
+        else:
+            rs = ref
         rd = rs.to_device(dev)
-        out = tuple(torch.empty((max(rs.n, 1024), qs.n), dtype=t, device=dev)
+        t0 = base["tile_spectra"]
+        tiles = sorted({max(32, min(MAX_AUTO_TILE, (int(t) + 31) // 32 * 32))
+                        for t in (t0 / 2, 0.75 * t0, t0, 1.5 * t0, 2 * t0)})
+        nq_max = min(qry.n, tiles_per_trial * max(tiles))
+        out = tuple(torch.empty((max(rs.n, class_sample), nq_max), dtype=t, device=dev)
                     for t in (torch.float32, torch.int32, torch.uint8))
 
-        def timed(rdev, n_rows, cfg):
-            o = tuple(t[:n_rows] for t in out)
-            run = lambda: kernels.cosine_greedy_dense(rdev, qd, tolerance, shift,  # noqa: E731
+        def timed(rdev, n_rows, qdev, n_q, cfg):
+            o = tuple(x[:n_rows, :n_q] for x in out)
+            run = lambda: kernels.cosine_greedy_dense(rdev, qdev, tolerance, shift,  # noqa: E731
                                                       match_limit, out=o, config=cfg)
             run()
             torch.cuda.synchronize()
@@ -222,24 +232,26 @@ class Tuner:
             return e0.elapsed_time(e1) / reps
 
         # 1) tile size: the estimate and its neighbours (at most MAX_AUTO_TILE:
-        # larger tiles cost the join a CTA per SM)
-        t0 = base["tile_spectra"]
-        tiles = sorted({max(32, min(MAX_AUTO_TILE, (int(t) + 31) // 32 * 32))
-                        for t in (t0 / 2, 0.75 * t0, t0, 1.5 * t0, 2 * t0)})
-        best_tile, best_ms = t0, float("inf")
+        # larger tiles cost the join a CTA per SM), tiles_per_trial tiles each
+        best_tile, best_ns = t0, float("inf")
         for t in tiles:
-            ms = timed(rd, rs.n, dict(base, tile_spectra=t))
-            report["trials"].append({"tile_spectra": t, "ms": ms})
-            if ms < best_ms:
-                best_tile, best_ms = t, ms
-        tile = min(best_tile, max(32, qs.n))
+            n_q = min(qry.n, tiles_per_trial * t)
+            qs = qry.subset(0, n_q)
+            ms = timed(rd, rs.n, qs.to_device(dev), n_q, dict(base, tile_spectra=t))
+            ns_pair = 1e6 * ms / (rs.n * n_q)
+            report["trials"].append({"tile_spectra": t, "ms": ms, "ns_per_pair": ns_pair})
+            if ns_pair < best_ns:
+                best_tile, best_ns = t, ns_pair
+        tile = min(best_tile, max(32, qry.n))
+        n_q = min(qry.n, tiles_per_trial * tile)
+        qd = qry.subset(0, n_q).to_device(dev)
         # 2) first sub-range width per reference length class
         widths = [0] * 17
         for c in range(17):
             members = np.nonzero(classes == c)[0]
             if members.size < 16:
                 continue
-            sel = np.sort(rng.choice(members, min(members.size, 1024), replace=False))
+            sel = np.sort(rng.choice(members, min(members.size, class_sample), replace=False))
             sub = ref.take(sel)
             sd = sub.to_device(dev)
             options = [0] + sorted({max(32, (tile // d) // 32 * 32) for d in (1, 2, 4, 8)},
@@ -248,7 +260,7 @@ class Tuner:
             for w in options:
                 wbc = [0] * 17
                 wbc[c] = w
-                ms = timed(sd, sub.n, dict(base, tile_spectra=tile, width_by_class=wbc))
+                ms = timed(sd, sub.n, qd, n_q, dict(base, tile_spectra=tile, width_by_class=wbc))
                 res.append((ms, w))
                 report["trials"].append({"class": c, "width": w, "ms": ms})
             ms0 = res[0][0]

@@ -37,7 +37,9 @@ def _raise_device_error(bits: int, what: str) -> None:
         parts.append("spectrum offsets are not non-decreasing within the peak arrays")
     if bits & _native.DEVERR_SPILL_OVERRUN:
         parts.append("spill list overrun")
-    raise NativeError(f"{what}: device reported bad input ({'; '.join(parts)})",
+    if bits & _native.DEVERR_PIPELINE_TIMEOUT:
+        parts.append("a bounded wait between the pair kernel's warps ran out")
+    raise NativeError(f"{what}: device reported an error ({'; '.join(parts)})",
                       _native.CMS_ERR_DEVICE)
 
 

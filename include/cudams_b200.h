@@ -75,8 +75,10 @@ int cms_destroy(cms_ctx* ctx);
 /*
  * Read and clear the context's device error word (synchronises `stream`).
  * Kernels set bits in it instead of faulting when they meet input that
- * breaks a precondition (a spectrum longer than CMS_MAX_PEAKS, a sparse
- * spill list overrun).  *bits receives the word (host pointer).
+ * breaks a precondition: 1 a spectrum longer than CMS_MAX_PEAKS, 2 a sparse
+ * spill list overrun, 4 bad offsets; and 8 when a bounded wait between the
+ * pipelined pair kernel's warps ran out (2 s; the kernel then stops early
+ * and its results are incomplete).  *bits receives the word (host pointer).
  */
 int cms_take_device_error(cms_ctx* ctx, uint32_t* bits, void* stream);
 

@@ -86,7 +86,8 @@ def test_measured_tuner_config(cuda_device, tmp_path):
     ref = synthetic.lognormal_spectra(3000, seed=15)
     qry = synthetic.lognormal_spectra(2500, seed=16)
     t = autotune.Tuner(str(tmp_path / "tune.json"))
-    cfg, report = t.measure(ref, qry, 0.01, 0.0, 4096, sample_ref=1000, sample_qry=2500)
+    cfg, report = t.measure(ref, qry, 0.01, 0.0, 4096, device=cuda_device, sample_ref=1000,
+                            tiles_per_trial=2)  # a torch.device, as bench.py passes it
     assert cfg["mode"] == 1 and len(cfg["width_by_class"]) == 17
     assert report["trials"] and report["buckets"]
     st = autotune.workload_stats(ref, qry, 0.01)
