@@ -1749,13 +1749,13 @@ int make_plan(const CosineArgs& args, const cms_cosine_config* cfg, bool sparse,
     if (cfg && cfg->tile_spectra > 0) {
         p.tile = cfg->tile_spectra;
     } else {
-        // about 128 expected candidates per work item (reference x tile) when
+        // about 200 expected candidates per work item (reference x tile) when
         // the caller gives candidates per pair, else 1024 queries; at most one
         // item per 100000 pairs so that every resident warp gets tens of items
         const long long pairs = (long long)args.ref.n * (long long)args.qry.n;
         long long t = 1024;
         if (cfg && cfg->cand_per_pair > 0.0)
-            t = (long long)std::min(2048.0, 128.0 / cfg->cand_per_pair);
+            t = (long long)std::min(2048.0, 200.0 / cfg->cand_per_pair);
         t = std::min(t, pairs / 100000);
         t = std::max<long long>(32, std::min<long long>(2048, t));
         p.tile = (int)((t + 31) / 32 * 32);

@@ -107,10 +107,10 @@ def workload_stats(ref: PackedSpectra, qry: PackedSpectra, tolerance: float,
 # problems still fill the GPU and the last items do not leave it idle
 TARGET_ITEMS = 100_000
 # expected candidates per work item: measured on B200 with lognormal spectra
-# (tol 0.01, ~0.1 candidates per pair) the time per pair is flat within 3%
-# between ~100 and ~180 candidates per item from 20k x 20k to 100k x 100k
-# (tiles 1024-1792); below ~75 the per-peak bucket lookups dominate
-CANDIDATES_PER_ITEM = 128.0
+# (tol 0.01, ~0.1 candidates per pair, 100k x 100k, whole query tiles) the
+# time per pair falls from 7.75 ps at ~130 candidates per item (1312 queries)
+# to 7.09 ps at ~200 (2048); below ~75 the per-peak bucket lookups dominate
+CANDIDATES_PER_ITEM = 200.0
 # largest automatic tile: the join's per-warp query counters grow with the
 # tile, and above ~2300 queries three CTAs no longer fit an SM
 MAX_AUTO_TILE = 2048

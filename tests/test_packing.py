@@ -167,6 +167,6 @@ def test_mean_candidates_estimate_matches_exact_mean():
     exact /= r.n * q.n
     est = autotune.mean_candidates(r, q, 0.01)
     assert abs(est - exact) / exact < 0.05, (est, exact)
-    # the heuristic turns it into ~128 candidates per work item
+    # the heuristic turns it into ~CANDIDATES_PER_ITEM candidates per work item
     cfg = autotune.heuristic_config(autotune.WorkloadStats(est, 0.0, 99.0, 99.0), 100_000, 100_000)
     assert abs(cfg["tile_spectra"] * est - autotune.CANDIDATES_PER_ITEM) < 32 * est + 1
