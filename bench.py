@@ -59,11 +59,11 @@ BYTES_PER_PAIR = 9
 # DRAM bytes per pair of join_kernel (read + write), from an ncu capture of the
 # 20k x 20k case of this workload (profiles/join_kernel_batched_cosine_20k.txt);
 # traffic grows with pairs, so a full launch is scaled by its pair count.
-JOIN_TRAFFIC_BYTES_PER_PAIR = 10.54
-# issue and shared-pipe utilisation of the same capture (quoted, not measured
-# by a bench run)
+JOIN_TRAFFIC_BYTES_PER_PAIR = 11.37
+# issue activity and the long-scoreboard share of stalls in the same capture
+# (quoted, not measured by a bench run)
 JOIN_PROFILE = "profiles/join_kernel_batched_cosine_20k.txt (20k x 20k capture)"
-JOIN_PROFILE_FIGURES = {"issue_active_pct": 47.2, "shared_pipe_pct": 21.0}
+JOIN_PROFILE_FIGURES = {"issue_active_pct": 38.5, "long_scoreboard_stall_pct": 40.0}
 
 
 def parse():

@@ -268,11 +268,12 @@ int cms_modified_cosine_sparse(cms_ctx* ctx, const float* ref_mz, const double* 
  * `stream`) and freed by cms_library_destroy.  cfg (may be NULL) sets the
  * library tile size / bucket width and the expected candidates per pair.
  * Searches on different contexts and streams may run concurrently against
- * one library (it is read-only after creation).  A search launches
- * short-lived CTAs (each warp takes a few work items and exits), so that the
- * SMs free up continuously and searches on other streams -- give urgent ones
- * a higher stream priority -- are scheduled in between: concurrent searches
- * overlap on the device.  Hit buffers and hit_count
+ * one library (it is read-only after creation).  A search launches four
+ * waves of short-lived CTAs (each warp takes an equal share of the work items
+ * and exits; each CTA borrows a slice of the context's candidate pool while
+ * it lives), so that the SMs free up continuously and searches on other
+ * streams -- give urgent ones a higher stream priority -- are scheduled in
+ * between: concurrent searches overlap on the device.  Hit buffers and hit_count
  * follow cms_cosine_greedy_sparse (hit_ref = library index, hit_query =
  * query index).
  */
