@@ -24,7 +24,7 @@ def P(tol, ml, shift=0.0):
     return {"tolerance": tol, "shift": shift, "match_limit": ml}
 
 
-@pytest.mark.parametrize("n", [301, 336, 384])  # 336, 384: 16-aligned rows (vector mirror)
+@pytest.mark.parametrize("n", [301, 336, 384])  # 336, 384: 16-aligned rows
 def test_dense_symmetric_differs_from_full_and_matches_oracle(cuda_device, n):
     from cudams import synthetic
 
@@ -121,3 +121,29 @@ def test_matrix_is_symmetric_numpy_sparse_and_blocked(cuda_device):
 
     with pytest.raises(ValueError, match="is_symmetric"):
         k.matrix(ref, synthetic.uniform_spectra(139, seed=72), is_symmetric=True)
+
+
+@pytest.mark.parametrize("cfg", [{}, {"mode": 2}, {"mode": 1, "tile_spectra": 64}])
+def test_dense_symmetric_into_stale_pitched_output(cuda_device, cfg):
+    """Symmetric dense results written from both sides of the diagonal into
+    output buffers with a row pitch above n that hold stale values: every
+    pair is written (no stale value survives) and the pitch padding keeps its
+    contents."""
+    import torch
+
+    from cudams import kernels, synthetic
+
+    dev = cuda_device
+    n, ld = 203, 211
+    s = synthetic.uniform_spectra(n, seed=44)
+    want = oracle.cosine_greedy_symmetric(s, s, 0.1, 0.0, 2048)
+    bufs = (torch.full((n, ld), 7.0, dtype=torch.float32, device=dev),
+            torch.full((n, ld), 99, dtype=torch.int32, device=dev),
+            torch.full((n, ld), 3, dtype=torch.uint8, device=dev))
+    sd = s.to_device(dev)
+    kernels.cosine_greedy_dense(sd, sd, 0.1, 0.0, 2048, out=tuple(b[:, :n] for b in bufs),
+                                config=dict(cfg, symmetric=1), check_errors=True)
+    got = tuple(b.cpu().numpy() for b in bufs)
+    assert_same(tuple(g[:, :n] for g in got), want, str(cfg))
+    assert (got[0][:, n:] == 7.0).all() and (got[1][:, n:] == 99).all()
+    assert (got[2][:, n:] == 3).all()
