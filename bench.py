@@ -31,8 +31,8 @@ CUDA kernel (installed under baseline/_ref) is timed beside ours on the
 1024 x 1024 workload (other_workloads.uniform_1k.reference_numba_kernel).
 
 --only NAME runs one of the other workloads alone (fingerprint, symmetric,
-uniform, overflow) and prints its result dict: the command profiler
-captures of those kernels use.
+uniform, overflow, modified) and prints its result dict: the command
+profiler captures of those kernels use.
 """
 from __future__ import annotations
 
@@ -84,7 +84,8 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--overflow-rows", type=int, default=1000,
                     help="reference rows of the overflow-stress sample (20000: the whole matrix)")
-    ap.add_argument("--only", choices=["fingerprint", "symmetric", "uniform", "overflow"],
+    ap.add_argument("--only", choices=["fingerprint", "symmetric", "uniform", "overflow",
+                                       "modified"],
                     default="", help="run only this one of the other workloads (for profiler "
                                      "captures) and print its result instead of the bench line")
     return ap.parse_args()
@@ -616,10 +617,11 @@ def _time_ms(fn, reps=3):
 def other_workloads(dev, args, only=""):
     """The other workloads, each bounded to seconds: device-resident pairs/s.
     only: run just the named one ("fingerprint", "symmetric", "uniform",
-    "overflow")."""
+    "overflow", "modified")."""
     res = {}
     for name, fn in (("fingerprint", _fingerprint_workload), ("symmetric", _symmetric_workload),
-                     ("uniform", _uniform_workload), ("overflow", _overflow_workload)):
+                     ("uniform", _uniform_workload), ("overflow", _overflow_workload),
+                     ("modified", _modified_workload)):
         if only in ("", name):
             res.update(fn(dev, args))
     return res
@@ -664,6 +666,25 @@ def _fingerprint_workload(dev, args):
     tms = _time_ms(torch_jaccard)
     del R, Q
     torch.cuda.empty_cache()
+    # the same torch formulation on the host cores (the reference's CPU
+    # fingerprint path), on a 4096 x 4096 tile
+    nc = min(4096, n_fp)
+    Rc = torch.from_numpy(np.unpackbits(bits[:nc].view(np.uint8), axis=1,
+                                        bitorder="little")).float()
+    Qc = torch.from_numpy(np.unpackbits(bits[n_fp:n_fp + nc].view(np.uint8), axis=1,
+                                        bitorder="little")).float()
+
+    def torch_cpu_jaccard():
+        inter = Rc @ Qc.T
+        u = Rc.sum(1, keepdim=True) + Qc.sum(1, keepdim=True).T
+        u -= inter
+        return inter.div(u).nan_to_num()
+
+    torch_cpu_jaccard()
+    t0 = time.perf_counter()
+    torch_cpu_jaccard()
+    cpu_s = time.perf_counter() - t0
+    del Rc, Qc
     # tensor-core kernel: 2 int8 ops (multiply, add) per bit per pair; the
     # int8 reference is twice the measured dense bf16 rate (the ratio of the
     # nominal dense figures, 4.5 POPS : 2.25 PFLOP/s; no int8 GEMM is measured)
@@ -682,6 +703,8 @@ def _fingerprint_workload(dev, args):
                      "hbm_frac_output": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
         "reference_torch_cuda_jaccard_pairs_per_s": nt * nt / (tms / 1e3),
         "reference_torch_sample": f"{nt} x {nt}",
+        "reference_torch_cpu_jaccard_pairs_per_s": nc * nc / cpu_s,
+        "reference_torch_cpu_sample": f"{nc} x {nc}, {torch.get_num_threads()} threads",
         "symmetric_jaccard_output_pairs_per_s": n_fp * n_fp / (ms_sym / 1e3)}
     return res
 
@@ -776,6 +799,40 @@ def _uniform_workload(dev, args):
                                      "numpy structured array (packing + H2D + kernels + D2H)"}}
 
     return res
+
+
+def _modified_workload(dev, args):
+    """Modified cosine (matchms ModifiedCosine) on 20k x 20k analogue families
+    (shared peaks shifted by precursor differences), beside greedy cosine on
+    the same spectra."""
+    import torch
+
+    from cudams import autotune, kernels, synthetic
+
+    n = min(args.n, 20_000)
+    r, rp = synthetic.analog_spectra(n, seed=args.seed + 20)
+    q, qp = synthetic.analog_spectra(n, seed=args.seed + 21)
+    cfg = autotune.choose_config(r, q, TOL)
+    mcfg = dict(cfg)
+    if mcfg.get("cand_per_pair"):  # the shifted pass adds about as many again
+        mcfg["cand_per_pair"] = 2.0 * mcfg["cand_per_pair"]
+        mcfg["tile_spectra"] = max(32, (mcfg.get("tile_spectra", 64) // 2 + 31) // 32 * 32)
+    rd, qd = r.to_device(dev), q.to_device(dev)
+    rpd, qpd = torch.from_numpy(rp).to(dev), torch.from_numpy(qp).to(dev)
+    out = tuple(torch.empty((n, n), dtype=t, device=dev)
+                for t in (torch.float32, torch.int32, torch.uint8))
+    ms_m = _time_ms(lambda: kernels.modified_cosine_dense(rd, rpd, qd, qpd, TOL, 2048, out=out,
+                                                          config=mcfg))
+    ms_c = _time_ms(lambda: kernels.cosine_greedy_dense(rd, qd, TOL, 0.0, 2048, out=out,
+                                                        config=cfg))
+    del out
+    torch.cuda.empty_cache()
+    return {"modified_cosine_20k": {
+        "workload": f"{n} x {n} analogue families (8 per family, precursor shifts U(-40, 40)), "
+                    f"tol {TOL}, match_limit 2048",
+        "modified_pairs_per_s": n * n / (ms_m / 1e3), "modified_ms": ms_m,
+        "greedy_cosine_pairs_per_s_same_spectra": n * n / (ms_c / 1e3),
+        "tuning": mcfg}}
 
 
 def _overflow_workload(dev, args):
