@@ -1,6 +1,8 @@
 // Context, errors and scratch management of libcudams_b200.so.
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -10,6 +12,11 @@
 namespace cms {
 
 static thread_local std::string g_last_error;
+
+int test_stall(const char* role) {
+    const char* v = std::getenv("CMS_TEST_STALL");
+    return (v && role && std::strcmp(v, role) == 0) ? 1 : 0;
+}
 
 void set_error(const char* fmt, ...) {
     char buf[512];

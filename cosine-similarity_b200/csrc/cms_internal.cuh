@@ -151,6 +151,12 @@ int raise_func_smem(const void* func, size_t bytes);
 // use in a kernel, else CMS_ERR_INVALID with a message naming `what`.
 int check_device_ptr(const void* p, const char* who, const char* what);
 
+// Test hook: nonzero when the environment variable CMS_TEST_STALL names
+// `role` ("mma": the fingerprint kernel's MMA issuer, "pair": the pipelined
+// pair kernel's greedy warp).  That role then does nothing, so the other
+// roles' bounded waits run out and the kernel's error path is exercised.
+int test_stall(const char* role);
+
 // Scope that counts `n` launches for a profiling stage and, when profiling
 // is on, records an event pair around them on stream `s`.
 class StageScope {

@@ -1172,6 +1172,9 @@ struct PairParams {
     uint32_t* err;
     const uint32_t* bad;
     int sym;  // only pairs (reference i, query j) with i <= j
+    // test hook (CMS_TEST_STALL=pair): the pipelined kernel's greedy warp
+    // leaves at once, so the producers' bounded waits run out
+    int test_stall;
 };
 
 // Register-blocked bitonic sort of m = 8 * blockDim.x candidates, descending by
@@ -1673,7 +1676,7 @@ __global__ void pair_kernel_pipe(PairParams P) {
                 ph ^= 1u;
             }
         }
-    } else {
+    } else if (!P.test_stall) {
         // consumer warp
         const int lane = tid & 31;
         int b = 0;
@@ -1994,6 +1997,7 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
                                     : pair_kernel_pipe<false, false>);
         const size_t pipe_smem = pair_smem + (size_t)p.cap * 12;
         const int pipe_threads = p.pair_threads + 32;
+        pp.test_stall = test_stall("pair");
         if ((rc = set_func_smem(pipe_k, pipe_smem))) return rc;
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipe_k, pipe_threads, pipe_smem);

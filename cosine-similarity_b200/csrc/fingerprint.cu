@@ -33,6 +33,10 @@ struct FpParams {
     float* out;
     int64_t ld;
     int sym;  // only outputs (i, j) with i <= j (n_r == n_q)
+    // test hook (environment variable CMS_TEST_STALL=mma): the MMA issuer
+    // issues nothing, so the producers' and the epilogue's bounded waits run
+    // out and the error path (abort flag, error bit, TMEM release) is taken
+    int test_stall;
 };
 
 template <int MEASURE>
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 1) fp_umma_kernel(FpParams P, Geomet
             int stage = 0;
             uint32_t phase = 0;
             int64_t it = 0;
-            bool ok = true;
+            bool ok = !P.test_stall;
             for (int64_t t = blockIdx.x; t < G.n_tiles && ok; t += gridDim.x) {
                 int tm, tn;
                 if (!tile_live(P, G, t, tm, tn)) continue;
@@ -587,7 +591,8 @@ int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
         set_error("%s: null pointer", who);
         return CMS_ERR_INVALID;
     }
-    FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld, sym};
+    FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld, sym,
+               test_stall("mma")};
     cudaStream_t s = (cudaStream_t)stream;
     int dev = 0, sms = 148;
     CMS_CUDA_TRY(cudaGetDevice(&dev));
