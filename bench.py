@@ -225,6 +225,16 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def lane_issue_frac(dev, visits_per_s: float) -> dict:
+    """Greedy-cosine lane-issue roofline: peak visits per second of a two-pointer
+    sweep of every pair, sum over pairs of (n_ref + n_query), against one
+    visit per lane per clock (SMs x 128 lanes x max SM clock)."""
+    mhz, src = sm_max_mhz()
+    peak = sm_count(dev) * 128 * mhz * 1e6
+    return {"achieved_visits_per_s": visits_per_s, "peak_visits_per_s": peak,
+            "frac": visits_per_s / peak, "peak_basis": f"SMs x 128 lanes x {mhz:.0f} MHz ({src})"}
+
+
 def measured_bf16_tflops():
     """Dense bf16 GEMM throughput (burst) from MEASURED_PEAKS.json, else the
     pool's fallback figure."""
@@ -700,7 +710,10 @@ def _fingerprint_workload(dev, args):
                      "peak_int8_ops_per_s": int8_peak,
                      "frac": ops_per_pair * fp["jaccard"] / int8_peak,
                      "peak_source": f"2 x {bf16_kind} bf16_tflops (dense int8 : bf16 = 2 : 1)",
-                     "hbm_frac_output": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9)},
+                     "hbm_frac_output": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9),
+                     # (4 R Q + 256 (R + Q)) bytes per measure over the measured copy rate
+                     "hbm_frac": (4.0 * n_fp * n_fp + 256.0 * 2 * n_fp) / (n_fp * n_fp / fp["jaccard"])
+                                 / (measured_peaks()[0] * 1e9)},
         "reference_torch_cuda_jaccard_pairs_per_s": nt * nt / (tms / 1e3),
         "reference_torch_sample": f"{nt} x {nt}",
         "reference_torch_cpu_jaccard_pairs_per_s": nc * nc / cpu_s,
@@ -786,8 +799,10 @@ def _uniform_workload(dev, args):
                                       2048, 1024, 1024)
     except Exception as e:  # noqa: BLE001 - reported, not fatal
         ref_k = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+    u_visits = 1024.0 * (u_r.n_peaks + u_q.n_peaks)  # sum over pairs of (n_ref + n_query)
     res["uniform_1k"] = {"workload": "1024 x 1024, peaks U{10..200}, tol 0.1, match_limit 2048",
                          "tiled_pairs_per_s": 1024 * 1024 / (ms_t / 1e3),
+                         "lane_issue_equivalent": lane_issue_frac(dev, u_visits / (ms_t / 1e3)),
                          "tiled_graph_pairs_per_s": 1024 * 1024 / (ms_g / 1e3),
                          "plain_pairs_per_s": 1024 * 1024 / (ms_p / 1e3),
                          "reference_numba_kernel": ref_k, "tiled_ms": ms_t,
@@ -862,6 +877,8 @@ def _overflow_workload(dev, args):
         "workload": "20k x 20k clustered (200 centres, sigma 0.02), 1000-2000 peaks, tol 0.05, "
                     "powers (3, 0.6), match_limit 1024",
         "tiled_pairs_per_s": rows * c_q.n / (ms_o / 1e3), "tiled_sample": f"{rows} x {c_q.n}",
+        "lane_issue_equivalent": lane_issue_frac(
+            dev, (c_q.n * float(c_r.lengths[:rows].sum()) + rows * float(c_q.n_peaks)) / (ms_o / 1e3)),
         "plain_pairs_per_s": prow * c_q.n / (ms_pl / 1e3), "plain_sample": f"{prow} x {c_q.n}",
         "overflow_fraction": ovf, "tuning": cfg}
     return res
