@@ -1368,6 +1368,137 @@ __device__ int gen_pair(const PairParams& P, int64_t ri, int64_t qi, unsigned lo
     return total;
 }
 
+// the in-thread stages of sort8_words (exchange distance J < 8)
+template <int J>
+__device__ __forceinline__ void words_local(unsigned long long (&c)[8], int base, int kk) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        if (e & J) continue;
+        const int f = e | J;
+        const bool desc = ((base + e) & kk) == 0;
+        const bool gt = c[e] > c[f];
+        if (desc ? !gt : gt) {
+            const unsigned long long t = c[e];
+            c[e] = c[f];
+            c[f] = t;
+        }
+    }
+}
+
+// Register-blocked bitonic sort, descending, of m = 8 * nt single 64-bit words
+// (thread t holds 8t..8t+7), exchanging through `scratch` (m words) for
+// distances of 256 and more; the sorted words end in `scratch`.
+template <typename Sync>
+__device__ void sort8_words(unsigned long long* scratch, unsigned long long (&c)[8], int m,
+                            int nt, int tid, Sync sync) {
+    const int base = 8 * tid;
+    const unsigned full = 0xffffffffu;
+    for (int kk = 2; kk <= m; kk <<= 1) {
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            if (j >= 8) {
+                const int pt = tid ^ (j >> 3);
+                const bool lower = (base & j) == 0;
+                const bool desc = (base & kk) == 0;
+                unsigned long long o[8];
+                if (j >= 256) {
+                    sync();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) scratch[e * nt + tid] = c[e];
+                    sync();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) o[e] = scratch[e * nt + pt];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) o[e] = __shfl_xor_sync(full, c[e], j >> 3);
+                }
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const bool gt = c[e] > o[e];
+                    if ((lower == desc) ? !gt : gt) c[e] = o[e];
+                }
+            } else if (j == 4) {
+                words_local<4>(c, base, kk);
+            } else if (j == 2) {
+                words_local<2>(c, base, kk);
+            } else {
+                words_local<1>(c, base, kk);
+            }
+        }
+    }
+    sync();
+#pragma unroll
+    for (int e = 0; e < 8; ++e) scratch[base + e] = c[e];
+    sync();
+}
+
+// Sorts the m = 8 * nt candidates of okey/cgen (padded past n with zeros)
+// into greedy order by sorting one 64-bit word per candidate: the order key
+// without its top bit (set for every key >= +0.0) and without its low R + 1
+// bits, then a "real candidate" bit, then the R-bit index (m = 2^R), so
+// equal words' order is the index order, i.e. generation order, and padding
+// sorts last.  Keys that agree in every kept bit but differ in a dropped one
+// would be misordered: the pass checks every pair of neighbours for that
+// (and for a key below +0.0) and returns false, leaving okey/cgen untouched,
+// if it finds one; the caller then sorts the pairs themselves.  On success
+// okey/cgen hold the candidates in greedy order.
+template <typename Sync>
+__device__ bool sort8_by_word(unsigned long long* okey, uint32_t* cgen,
+                              unsigned long long* scratch, int* s_flag, int n, int m, int nt,
+                              int tid, Sync sync) {
+    const int rb = 31 - __clz(m);  // index bits
+    const unsigned long long imask = (1ull << rb) - 1ull;
+    const unsigned long long real = 1ull << rb;
+    const unsigned long long kmask = ~((real << 1) - 1ull);
+    if (tid == 0) *s_flag = 0;
+    sync();
+    unsigned long long c[8];
+    bool bad = false;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const int i = 8 * tid + e;
+        if (i < n) {
+            const unsigned long long k = okey[i];
+            bad |= (k >> 63) == 0ull;
+            c[e] = ((k << 1) & kmask) | real | (unsigned long long)i;
+        } else {
+            c[e] = (unsigned long long)i;  // padding: below every real word
+        }
+    }
+    if (bad) atomicOr(s_flag, 1);
+    sort8_words(scratch, c, m, nt, tid, sync);
+    // neighbours that tie in the kept bits must have equal keys
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const int i = 8 * tid + e;
+        if (i + 1 < m && (c[e] & real)) {
+            const unsigned long long nx = e < 7 ? c[e + 1] : scratch[i + 1];
+            if ((nx & real) && ((nx ^ c[e]) & kmask) == 0ull &&
+                okey[nx & imask] != okey[c[e] & imask])
+                bad = true;
+        }
+    }
+    if (bad) atomicOr(s_flag, 1);
+    sync();
+    if (*s_flag) return false;
+    unsigned long long k[8];
+    uint32_t g[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const bool r = (c[e] & real) != 0ull;
+        const int src = (int)(c[e] & imask);
+        k[e] = r ? okey[src] : 0ull;
+        g[e] = r ? cgen[src] : 0u;
+    }
+    sync();
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        okey[8 * tid + e] = k[e];
+        cgen[8 * tid + e] = g[e];
+    }
+    sync();
+    return true;
+}
+
 // Pads okey/cgen[n, m) and sorts [0, m) descending by (okey, gen), m the
 // power of two >= n: in registers when m = 8 * nt, else in shared memory.
 template <typename Sync>
@@ -1606,7 +1737,10 @@ __global__ void pair_kernel_pipe(PairParams P) {
     uint32_t* cgen0 = reinterpret_cast<uint32_t*>(okey0 + 2 * P.cap);
     uint32_t* used_r = cgen0 + 2 * P.cap;  // 2048 words: 65536 peaks
     uint32_t* used_q = used_r + 2048;
+    // the producers' sort scratch: one 64-bit word per candidate slot
+    unsigned long long* scratch = reinterpret_cast<unsigned long long*>(used_q + 2048);
     __shared__ int s_scan[32];
+    __shared__ int s_flag;
     __shared__ unsigned long long s_item;
     __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
     __shared__ long long s_ri[2], s_qi[2];
@@ -1662,7 +1796,11 @@ __global__ void pair_kernel_pipe(PairParams P) {
                 if (n > 0) {
                     int m = 1;
                     while (m < n) m <<= 1;
-                    sort_pair(okey, cgen, n, m, np, tid, sync);
+                    // one word per candidate when the pair fills the register
+                    // sort; the (key, gen) pairs themselves otherwise
+                    if (!(m == 8 * np &&
+                          sort8_by_word(okey, cgen, scratch, &s_flag, n, m, np, tid, sync)))
+                        sort_pair(okey, cgen, n, m, np, tid, sync);
                 }
             }
             if (tid == 0) {
@@ -1990,14 +2128,16 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     pair_blocks_per_sm = std::max(1, pair_blocks_per_sm);
     const int pair_grid = ctx->sm_count * pair_blocks_per_sm;
 
-    if (p.mode == 2 && pair_smem + (size_t)p.cap * 12 <= ctx->smem_optin) {
+    if (p.mode == 2 &&
+        pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 64 <= ctx->smem_optin) {
         // whole matrix: the pipelined pair kernel (pair_threads producers
         // plus a consumer warp, two candidate buffers)
         void (*pipe_k)(PairParams) =
             sparse ? (args.modified ? pair_kernel_pipe<true, true> : pair_kernel_pipe<true, false>)
                    : (args.modified ? pair_kernel_pipe<false, true>
                                     : pair_kernel_pipe<false, false>);
-        const size_t pipe_smem = pair_smem + (size_t)p.cap * 12;
+        // two candidate buffers and the sort's word scratch (8 per producer)
+        const size_t pipe_smem = pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 64;
         const int pipe_threads = p.pair_threads + 32;
         pp.test_stall = test_stall("pair");
         if ((rc = set_func_smem(pipe_k, pipe_smem))) return rc;
