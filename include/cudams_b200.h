@@ -330,9 +330,9 @@ int cms_cosine_greedy_noalloc(const float* ref_mz, const double* ref_a, const do
 /*
  * Fingerprint similarity on bit-packed fingerprints: n_words uint32 per
  * row, bit k in word k/32 at bit k%32, unused high bits zero.  The
- * intersection counts I = R . Q^T run on the tensor cores (tcgen05, 8-bit
- * integer operands expanded from the bits in shared memory, exact int32
- * accumulation).  Writes
+ * intersection counts I = R . Q^T run on the tensor cores (tcgen05
+ * kind::mxf4: 4-bit float operands of value 0 or 1 expanded from the bits in
+ * shared memory, block scale factors 1, exact float32 accumulation).  Writes
  * out[i*ld + j] (float32) for every (reference i, query j):
  *   CMS_FP_JACCARD  I / (a + b - I)      vector_similarity_functions.py:42-46
  *   CMS_FP_DICE     2 * (I / (a + b))    vector_similarity_functions.py:87-90
@@ -355,6 +355,18 @@ int cms_fingerprint(int measure, const uint32_t* ref_bits, const uint8_t* ref_va
  * of the calls since the last read are not valid.
  */
 int cms_fingerprint_take_error(uint32_t* bits, void* stream);
+
+/*
+ * Self-check of the fingerprint epilogue's branch-free float32 division and
+ * square root against CUDA's IEEE operations, bit for bit, on the device.
+ * No reference counterpart.  Writes five mismatch counts to the host array
+ * `mismatches` (synchronises `stream`): [0] n / d for all integers
+ * 0 <= n <= d <= 65536; [1] sqrt(p) and [2] the reciprocal of sqrt(p) for
+ * every float p in [1, 2^30]; [3] the cosine I / sqrt(a * b) for every
+ * a, b <= 2048 and I <= min(a, b); [4] the same for 2^30 pseudo-random
+ * triples with a, b <= 32768.  All five are 0 on a correct device.
+ */
+int cms_fingerprint_arith_check(uint64_t* mismatches, void* stream);
 
 /*
  * cms_fingerprint with matchms' is_symmetric=True (the reference's

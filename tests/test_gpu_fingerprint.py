@@ -100,6 +100,46 @@ def test_sizes_and_masks(cuda_device, n_bits, measure):
         _bits_equal(got, oracle.fingerprint(measure, rb, rv, qb, qv, rb.shape[1], fill))
 
 
+def test_branch_free_arithmetic_exhaustive(cuda_device):
+    """The epilogue's division and square root equal CUDA's IEEE ones, bit
+    for bit, over every operand the three measures can produce (and a 2^30
+    sample of the large-fingerprint cosine triples)."""
+    import ctypes
+
+    import torch
+
+    from cudams import _native
+
+    counts = (ctypes.c_uint64 * 5)()
+    with torch.cuda.device(cuda_device):
+        _native.check(_native.load().cms_fingerprint_arith_check(counts, None),
+                      "cms_fingerprint_arith_check")
+    assert list(counts) == [0, 0, 0, 0, 0]
+
+
+@pytest.mark.parametrize("n_bits", [16384, 32768])
+def test_exact_large_counts(cuda_device, n_bits):
+    """Nearly full fingerprints: intersection counts up to n_bits, odd ones
+    among them, so every bit of a 15-bit count must survive the tensor-core
+    accumulation exactly."""
+    rng = np.random.default_rng(n_bits + 1)
+    words = n_bits // 32
+    nr, nq = 40, 300
+
+    def rows(n):
+        b = np.full((n, words), 0xFFFFFFFF, dtype=np.uint32)
+        for i in range(1, n):  # row 0 stays full
+            drop = rng.choice(n_bits, size=int(rng.integers(1, 64)), replace=False)
+            np.bitwise_and.at(b[i], drop // 32, ~(np.uint32(1) << (drop % 32).astype(np.uint32)))
+        return b
+
+    rb, qb = rows(nr), rows(nq)
+    for measure in MEASURES:
+        got = _gpu(measure, rb, None, qb, None, words, np.nan)
+        _bits_equal(got, oracle.fingerprint(measure, rb, None, qb, None, words, np.nan))
+    assert _gpu("jaccard", rb[:1], None, qb[:1], None, words, np.nan)[0, 0] == 1.0
+
+
 def test_large_symmetric(cuda_device):
     """12k x 12k of the 2048-bit workload against itself: symmetric, diagonal 1,
     and 20k sampled entries equal to the oracle."""
