@@ -695,21 +695,25 @@ def _fingerprint_workload(dev, args):
     torch_cpu_jaccard()
     cpu_s = time.perf_counter() - t0
     del Rc, Qc
-    # tensor-core kernel: 2 int8 ops (multiply, add) per bit per pair; the
-    # int8 reference is twice the measured dense bf16 rate (the ratio of the
-    # nominal dense figures, 4.5 POPS : 2.25 PFLOP/s; no int8 GEMM is measured)
+    # tensor-core kernel: 2 ops (multiply, add) per bit per pair on 4-bit float
+    # operands (kind::mxf4); the fp4 reference is four times the measured dense
+    # bf16 rate (the ratio of the nominal dense figures, 9 PFLOP/s : 2.25; no
+    # fp4 GEMM is measured).  Neither the tensor pipe nor HBM bounds this
+    # kernel: the shared-memory traffic of the operand expansion, the tensor
+    # core's operand reads and the epilogue's staging does (see profiles/).
     bf16, bf16_kind = measured_bf16_tflops()
     ops_per_pair = 2 * 32 * bits.shape[1]
-    int8_peak = 2 * bf16 * 1e12
+    fp4_peak = 4 * bf16 * 1e12
     res["fingerprint_100k"] = {
         "workload": f"{n_fp} x {n_fp} fingerprints, 2048 bits, density U(5%,15%)",
         "pairs_per_s": fp, "unit": "pairs/s",
         "ms_per_measure": {m: n_fp * n_fp / v * 1e3 for m, v in fp.items()},
-        "roofline": {"bound": "tensor (int8)", "kernel": "fp_umma_kernel",
-                     "achieved_int8_ops_per_s": ops_per_pair * fp["jaccard"],
-                     "peak_int8_ops_per_s": int8_peak,
-                     "frac": ops_per_pair * fp["jaccard"] / int8_peak,
-                     "peak_source": f"2 x {bf16_kind} bf16_tflops (dense int8 : bf16 = 2 : 1)",
+        "roofline": {"bound": "shared memory (tensor fp4 and HBM fractions below)",
+                     "kernel": "fp_umma_kernel",
+                     "achieved_fp4_ops_per_s": ops_per_pair * fp["jaccard"],
+                     "peak_fp4_ops_per_s": fp4_peak,
+                     "frac": ops_per_pair * fp["jaccard"] / fp4_peak,
+                     "peak_source": f"4 x {bf16_kind} bf16_tflops (dense fp4 : bf16 = 4 : 1)",
                      "hbm_frac_output": 4 * fp["jaccard"] / (measured_peaks()[0] * 1e9),
                      # (4 R Q + 256 (R + Q)) bytes per measure over the measured copy rate
                      "hbm_frac": (4.0 * n_fp * n_fp + 256.0 * 2 * n_fp) / (n_fp * n_fp / fp["jaccard"])

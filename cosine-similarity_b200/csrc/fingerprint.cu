@@ -271,18 +271,37 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
             smem_u32(bar))
         : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+// Load 32 TMEM columns of this warp's 32 lanes (lane i: row i, r[j]: column
+// j) without waiting; tmem_wait_ld completes it.  The wait names the
+// destination registers as read-write operands, so the compiler can neither
+// read nor move them before the data has arrived, and the load overlaps
+// whatever the warp does in between.
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
         "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                   "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                   "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                   "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    tmem_ld32_async(taddr, r);
+    tmem_wait_ld(r);
 }
 
 // 2-D tensor store of one staged chunk (box 32 x 32 floats at column x, row
@@ -627,13 +646,23 @@ __global__ void __launch_bounds__(kThreads, 1)
             // the quarter's warps take every kEpiSets-th 32-column chunk,
             // starting one further on each tile, so that the odd chunk of
             // the 224 columns goes to each warp in turn
-            for (int c = (int)((set + it) % kEpiSets); c < kBN / 32; c += kEpiSets) {
+            // chunk c's accumulator columns are read (into vn) while chunk
+            // c - kEpiSets is computed and stored
+            uint32_t vn[32];
+            const uint32_t tbase =
+                tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccStride);
+            const int c0 = (int)((set + it) % kEpiSets);
+            __syncwarp();
+            if (c0 < kBN / 32) tmem_ld32(tbase + (uint32_t)(c0 * 32), vn);
+            for (int c = c0; c < kBN / 32; c += kEpiSets) {
                 const int col_l = c * 32;  // first column of this chunk in the tile
                 const int64_t gc0 = (int64_t)tn * kBN + col_l;
                 uint32_t v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = vn[j];
                 __syncwarp();
-                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kAccStride + col_l),
-                          v);
+                if (c + kEpiSets < kBN / 32)
+                    tmem_ld32_async(tbase + (uint32_t)((c + kEpiSets) * 32), vn);
                 const float* pbc = pb + acc * kBN + col_l;
                 // every row and column of the chunk has a fingerprint: no
                 // per-element fill test
@@ -704,6 +733,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                     }
                 }
+                tmem_wait_ld(vn);
             }
             __syncwarp();
             tc_fence_before();
@@ -829,6 +859,11 @@ int fingerprint_impl(const char* who, int measure, const uint32_t* ref_bits,
         set_error("%s: null pointer", who);
         return CMS_ERR_INVALID;
     }
+    // one set against itself (the same rows and flags): every measure is
+    // symmetric in (I, a, b), so the full matrix is the mirrored one bit for
+    // bit, and computing it costs less than half the tiles plus the mirror
+    // pass's transposed copy of the lower triangle
+    if (sym && ref_bits == q_bits && ref_valid == q_valid) sym = 0;
     FpParams P{ref_bits, ref_valid, n_ref, q_bits, q_valid, n_q, n_words, fill, out, ld, sym,
                test_stall("mma")};
     cudaStream_t s = (cudaStream_t)stream;

@@ -69,8 +69,16 @@ class CudaFingerprintSimilarity(BaseSimilarity):
         if qb.shape[1] != n_words:
             qb = np.zeros((qb.shape[0], n_words), np.uint32)
         t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
-        out = kernels.fingerprint_matrix(self.similarity_measure, t(rb), t(rv), t(qb), t(qv),
-                                         n_words, self._fill(), symmetric=symmetric)
+        r_bits, r_valid = t(rb), t(rv)
+        if symmetric and np.array_equal(rb, qb) and np.array_equal(rv, qv):
+            # one set against itself: the same device arrays on both sides let
+            # the library compute the full matrix directly (bit-identical to
+            # the mirrored one, and faster than half the tiles plus the mirror)
+            q_bits, q_valid = r_bits, r_valid
+        else:
+            q_bits, q_valid = t(qb), t(qv)
+        out = kernels.fingerprint_matrix(self.similarity_measure, r_bits, r_valid, q_bits,
+                                         q_valid, n_words, self._fill(), symmetric=symmetric)
         return out.cpu().numpy()
 
     def pair(self, reference, query) -> np.ndarray:
@@ -90,8 +98,9 @@ class CudaFingerprintSimilarity(BaseSimilarity):
         StackedSparseArray for array_type="sparse".
 
         is_symmetric=True (matchms semantics; the reference ignores the flag):
-        R == Q, pairs (i, j) with i <= j are computed and mirrored to (j, i),
-        which halves the popcount work."""
+        R == Q, pairs (i, j) with i <= j are computed and mirrored to (j, i);
+        for one set against itself the full matrix is computed directly (the
+        same values, and faster than half the tiles plus the mirror copy)."""
         fps_ref = [s.get("fingerprint") for s in references]
         fps_qry = [s.get("fingerprint") for s in queries]
         n_ref = sum(fp is not None for fp in fps_ref)

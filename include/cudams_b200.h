@@ -373,9 +373,11 @@ int cms_fingerprint_arith_check(uint64_t* mismatches, void* stream);
  * CudaFingerprintSimilarity.matrix accepts the flag and ignores it,
  * CudaFingerprintSimilarity.py:113-119): n references and n queries; only the
  * pairs (i, j) with i <= j are computed, as (reference i, query j), and
- * (j, i) receives the same value.  Half of the popcount work of
- * cms_fingerprint; for one set against itself the result is bit-identical
- * to it (every measure is symmetric in I, a and b).
+ * (j, i) receives the same value.  For one set against itself the result is
+ * bit-identical to cms_fingerprint (every measure is symmetric in I, a and
+ * b); when both sides are the same arrays (ref_bits == q_bits and ref_valid
+ * == q_valid) the full matrix is computed directly, which is faster than the
+ * upper triangle plus the mirror copy.
  */
 int cms_fingerprint_symmetric(int measure, const uint32_t* ref_bits, const uint8_t* ref_valid,
                               const uint32_t* q_bits, const uint8_t* q_valid, int64_t n,

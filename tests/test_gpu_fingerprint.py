@@ -178,6 +178,11 @@ def test_symmetric(cuda_device, measure, n):
     got = kernels.fingerprint_matrix(measure, t(a), t(va), t(a), t(va), n_words, np.nan,
                                      symmetric=True, check_errors=True).cpu().numpy()
     _bits_equal(got, full_aa)
+    # the same arrays on both sides: computed as the full matrix
+    ta, tva = t(a), t(va)
+    got = kernels.fingerprint_matrix(measure, ta, tva, ta, tva, n_words, np.nan,
+                                     symmetric=True, check_errors=True).cpu().numpy()
+    _bits_equal(got, full_aa)
 
     full_ab = oracle.fingerprint(measure, a, va, b, vb, n_words, -1.0)
     lower = np.tril_indices(n, -1)
