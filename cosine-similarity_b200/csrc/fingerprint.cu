@@ -636,9 +636,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int acc = (int)(it & 1);
             const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
             ++it;
-            if (!mbar_wait(&tfull[acc], acc_phase, abort_flag)) break;
+            // warp-uniform exits: the TMEM loads below are warp-collective
+            if (!__all_sync(0xFFFFFFFFu, mbar_wait(&tfull[acc], acc_phase, abort_flag))) break;
             tc_fence_after();
-            if (!mbar_wait(&pfull[acc], acc_phase, abort_flag)) break;
+            if (!__all_sync(0xFFFFFFFFu, mbar_wait(&pfull[acc], acc_phase, abort_flag))) break;
             const int row_l = quarter * 32 + lane;
             const float fa = pa[acc * kBM + row_l];
             const int64_t gr = (int64_t)tm * kBM + row_l;  // this lane's output row
