@@ -1386,8 +1386,9 @@ __device__ __forceinline__ void words_local(unsigned long long (&c)[8], int base
 }
 
 // Register-blocked bitonic sort, descending, of m = 8 * nt single 64-bit words
-// (thread t holds 8t..8t+7), exchanging through `scratch` (m words) for
-// distances of 256 and more; the sorted words end in `scratch`.
+// (thread t holds network positions 8t..8t+7), exchanging through `scratch`
+// (m words) for distances of 256 and more; the sorted words end in the
+// threads' registers, position 8t + e in c[e] of thread t.
 template <typename Sync>
 __device__ void sort8_words(unsigned long long* scratch, unsigned long long (&c)[8], int m,
                             int nt, int tid, Sync sync) {
@@ -1425,10 +1426,6 @@ __device__ void sort8_words(unsigned long long* scratch, unsigned long long (&c)
             }
         }
     }
-    sync();
-#pragma unroll
-    for (int e = 0; e < 8; ++e) scratch[base + e] = c[e];
-    sync();
 }
 
 // Sorts the m = 8 * nt candidates of okey/cgen (padded past n with zeros)
@@ -1453,9 +1450,12 @@ __device__ bool sort8_by_word(unsigned long long* okey, uint32_t* cgen,
     sync();
     unsigned long long c[8];
     bool bad = false;
+    // which candidate starts at which network position is free (every word
+    // carries its index): thread tid takes candidates e * nt + tid, so that
+    // the loads of consecutive threads are consecutive words
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-        const int i = 8 * tid + e;
+        const int i = e * nt + tid;
         if (i < n) {
             const unsigned long long k = okey[i];
             bad |= (k >> 63) == 0ull;
@@ -1466,12 +1466,17 @@ __device__ bool sort8_by_word(unsigned long long* okey, uint32_t* cgen,
     }
     if (bad) atomicOr(s_flag, 1);
     sort8_words(scratch, c, m, nt, tid, sync);
-    // neighbours that tie in the kept bits must have equal keys
+    // neighbours that tie in the kept bits must have equal keys; the word
+    // after this thread's last is the next thread's first
+    sync();
+    scratch[tid] = c[0];
+    sync();
+    const unsigned long long after = tid + 1 < nt ? scratch[tid + 1] : 0ull;
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const int i = 8 * tid + e;
         if (i + 1 < m && (c[e] & real)) {
-            const unsigned long long nx = e < 7 ? c[e + 1] : scratch[i + 1];
+            const unsigned long long nx = e < 7 ? c[e + 1] : after;
             if ((nx & real) && ((nx ^ c[e]) & kmask) == 0ull &&
                 okey[nx & imask] != okey[c[e] & imask])
                 bad = true;
@@ -1480,20 +1485,29 @@ __device__ bool sort8_by_word(unsigned long long* okey, uint32_t* cgen,
     if (bad) atomicOr(s_flag, 1);
     sync();
     if (*s_flag) return false;
+    // the sorted words to scratch, position p at p + p / 8 (the stores of
+    // positions 8 * tid + e, nine words apart, fall in different banks), then
+    // each thread gathers positions e * nt + tid, so that the final stores of
+    // consecutive threads are consecutive
+#pragma unroll
+    for (int e = 0; e < 8; ++e) scratch[9 * tid + e] = c[e];
+    sync();
     unsigned long long k[8];
     uint32_t g[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-        const bool r = (c[e] & real) != 0ull;
-        const int src = (int)(c[e] & imask);
+        const int pos = e * nt + tid;
+        const unsigned long long w = scratch[pos + (pos >> 3)];
+        const bool r = (w & real) != 0ull;
+        const int src = (int)(w & imask);
         k[e] = r ? okey[src] : 0ull;
         g[e] = r ? cgen[src] : 0u;
     }
     sync();
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-        okey[8 * tid + e] = k[e];
-        cgen[8 * tid + e] = g[e];
+        okey[e * nt + tid] = k[e];
+        cgen[e * nt + tid] = g[e];
     }
     sync();
     return true;
@@ -1737,7 +1751,8 @@ __global__ void pair_kernel_pipe(PairParams P) {
     uint32_t* cgen0 = reinterpret_cast<uint32_t*>(okey0 + 2 * P.cap);
     uint32_t* used_r = cgen0 + 2 * P.cap;  // 2048 words: 65536 peaks
     uint32_t* used_q = used_r + 2048;
-    // the producers' sort scratch: one 64-bit word per candidate slot
+    // the producers' sort scratch: one 64-bit word per candidate slot, and one
+    // more per eight (the padded layout of the sorted words)
     unsigned long long* scratch = reinterpret_cast<unsigned long long*>(used_q + 2048);
     __shared__ int s_scan[32];
     __shared__ int s_flag;
@@ -2129,7 +2144,7 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
     const int pair_grid = ctx->sm_count * pair_blocks_per_sm;
 
     if (p.mode == 2 &&
-        pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 64 <= ctx->smem_optin) {
+        pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 72 <= ctx->smem_optin) {
         // whole matrix: the pipelined pair kernel (pair_threads producers
         // plus a consumer warp, two candidate buffers)
         void (*pipe_k)(PairParams) =
@@ -2137,7 +2152,7 @@ int enqueue_cosine(cms_ctx* ctx, const CosineArgs& args, const DenseOut* dense,
                    : (args.modified ? pair_kernel_pipe<false, true>
                                     : pair_kernel_pipe<false, false>);
         // two candidate buffers and the sort's word scratch (8 per producer)
-        const size_t pipe_smem = pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 64;
+        const size_t pipe_smem = pair_smem + (size_t)p.cap * 12 + (size_t)p.pair_threads * 72;
         const int pipe_threads = p.pair_threads + 32;
         pp.test_stall = test_stall("pair");
         if ((rc = set_func_smem(pipe_k, pipe_smem))) return rc;
