@@ -31,7 +31,7 @@ CUDA kernel (installed under baseline/_ref) is timed beside ours on the
 1024 x 1024 workload (other_workloads.uniform_1k.reference_numba_kernel).
 
 --only NAME runs one of the other workloads alone (fingerprint, symmetric,
-uniform, overflow, modified) and prints its result dict: the command
+uniform, overflow, modified, metadata) and prints its result dict: the command
 profiler captures of those kernels use.
 """
 from __future__ import annotations
@@ -85,7 +85,7 @@ def parse():
     ap.add_argument("--overflow-rows", type=int, default=1000,
                     help="reference rows of the overflow-stress sample (20000: the whole matrix)")
     ap.add_argument("--only", choices=["fingerprint", "symmetric", "uniform", "overflow",
-                                       "modified"],
+                                       "modified", "metadata"],
                     default="", help="run only this one of the other workloads (for profiler "
                                      "captures) and print its result instead of the bench line")
     return ap.parse_args()
@@ -627,11 +627,11 @@ def _time_ms(fn, reps=3):
 def other_workloads(dev, args, only=""):
     """The other workloads, each bounded to seconds: device-resident pairs/s.
     only: run just the named one ("fingerprint", "symmetric", "uniform",
-    "overflow", "modified")."""
+    "overflow", "modified", "metadata")."""
     res = {}
     for name, fn in (("fingerprint", _fingerprint_workload), ("symmetric", _symmetric_workload),
                      ("uniform", _uniform_workload), ("overflow", _overflow_workload),
-                     ("modified", _modified_workload)):
+                     ("modified", _modified_workload), ("metadata", _metadata_workload)):
         if only in ("", name):
             res.update(fn(dev, args))
     return res
@@ -852,6 +852,48 @@ def _modified_workload(dev, args):
         "modified_pairs_per_s": n * n / (ms_m / 1e3), "modified_ms": ms_m,
         "greedy_cosine_pairs_per_s_same_spectra": n * n / (ms_c / 1e3),
         "tuning": mcfg}}
+
+
+def _metadata_workload(dev, args):
+    """matchms PrecursorMzMatch (Dalton and ppm) on 100k x 100k precursor
+    values (one byte per pair: output bandwidth) and IntersectMz on 20k x 20k
+    lognormal spectra with m/z rounded to 0.01 (so that exact matches occur)."""
+    import numpy as np
+    import torch
+
+    from cudams import kernels, synthetic
+
+    n = min(args.n, 100_000)
+    rng = np.random.default_rng(args.seed + 30)
+    rv = torch.from_numpy(rng.uniform(100.0, 1500.0, n)).to(dev)
+    qv = torch.from_numpy(rng.uniform(100.0, 1500.0, n)).to(dev)
+    out = torch.empty((n, n), dtype=torch.uint8, device=dev)
+    ms_d = _time_ms(lambda: kernels.mass_match_matrix(rv, qv, 0.1, False, out=out))
+    ms_p = _time_ms(lambda: kernels.mass_match_matrix(rv, qv, 20.0, True, out=out))
+    del out
+    torch.cuda.empty_cache()
+    m = min(args.n, 20_000)
+    sr = synthetic.lognormal_spectra(m, seed=args.seed + 31)
+    sq = synthetic.lognormal_spectra(m, seed=args.seed + 32)
+
+    def csr(s):
+        return (torch.from_numpy(np.round(s.mz.astype(np.float64), 2)).to(dev),
+                torch.from_numpy(s.offsets.astype(np.int64)).to(dev))
+
+    ix_out = torch.empty((m, m), dtype=torch.float64, device=dev)
+    (rm, ro), (qm, qo) = csr(sr), csr(sq)
+    ms_i = _time_ms(lambda: kernels.intersect_mz_matrix(rm, ro, qm, qo, 1.0, out=ix_out))
+    del ix_out
+    torch.cuda.empty_cache()
+    peak = measured_peaks()[0] * 1e9
+    return {"metadata_similarities": {
+        "workload": f"PrecursorMzMatch {n} x {n} (tolerance 0.1 Da / 20 ppm); IntersectMz "
+                    f"{m} x {m} lognormal spectra, m/z rounded to 0.01",
+        "precursor_match_dalton_pairs_per_s": n * n / (ms_d / 1e3),
+        "precursor_match_ppm_pairs_per_s": n * n / (ms_p / 1e3),
+        "precursor_match_hbm_frac": n * n / (ms_d / 1e3) / peak,
+        "intersect_mz_pairs_per_s": m * m / (ms_i / 1e3),
+        "intersect_mz_ms": ms_i}}
 
 
 def _overflow_workload(dev, args):

@@ -85,6 +85,9 @@ SIGNATURES = {
         c_int, _p, _p, c_int64, _p, _p, c_int64, c_int, c_float, _p, c_int64, _p]),
     "cms_fingerprint_take_error": (c_int, [POINTER(c_uint32), _p]),
     "cms_fingerprint_arith_check": (c_int, [POINTER(ctypes.c_uint64), _p]),
+    "cms_mass_match": (c_int, [_p, c_int64, _p, c_int64, c_double, c_int, _p, c_int64, _p]),
+    "cms_intersect_mz": (c_int, [
+        _p, _p, c_int64, c_int64, _p, _p, c_int64, c_int64, c_double, _p, c_int64, _p, _p]),
     "cms_fingerprint_symmetric": (c_int, [
         c_int, _p, _p, _p, _p, c_int64, c_int, c_float, _p, c_int64, _p]),
 }

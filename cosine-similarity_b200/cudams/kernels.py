@@ -295,3 +295,56 @@ def modified_cosine_sparse(ref: DeviceSpectra, ref_precursor, qry: DeviceSpectra
         if n <= cap:
             return SparseHits(*bufs, n)
         cap = n
+
+
+def mass_match_matrix(ref_values, q_values, tolerance: float, ppm: bool = False, *, out=None,
+                      stream=None):
+    """matchms ParentMassMatch / PrecursorMzMatch for all pairs -> uint8 (0/1)
+    [n_ref, n_q] on the device.  ref_values / q_values: float64 device
+    tensors (parent masses or precursor m/z); ppm selects the tolerance in
+    parts per million of the pair's mean."""
+    lib = _native.load()
+    device = ref_values.device
+    s = _stream(device, stream)
+    n_r, n_q = int(ref_values.shape[0]), int(q_values.shape[0])
+    if ref_values.dtype != torch.float64 or q_values.dtype != torch.float64:
+        raise TypeError("mass_match_matrix takes float64 values")
+    if out is None:
+        out = torch.empty((n_r, n_q), dtype=torch.uint8, device=device)
+    rc = lib.cms_mass_match(ptr(ref_values.contiguous()), n_r, ptr(q_values.contiguous()), n_q,
+                            float(tolerance), 1 if ppm else 0, ptr(out), int(out.stride(0)),
+                            stream_handle(s))
+    check(rc, "cms_mass_match")
+    return out
+
+
+def intersect_mz_matrix(ref_mz, ref_off, q_mz, q_off, scaling: float = 1.0, *, out=None,
+                        stream=None, check_errors: bool = False):
+    """matchms IntersectMz for all pairs -> float64 [n_ref, n_q] on the
+    device.  *_mz: float64 peak m/z (sorted within each spectrum), *_off:
+    int64 CSR offsets [n + 1], all device tensors."""
+    lib = _native.load()
+    device = ref_off.device
+    s = _stream(device, stream)
+    n_r, n_q = int(ref_off.shape[0]) - 1, int(q_off.shape[0]) - 1
+    for t, name in ((ref_mz, "ref_mz"), (q_mz, "q_mz")):
+        if t.dtype != torch.float64:
+            raise TypeError(f"{name} must be float64")
+    for t, name in ((ref_off, "ref_off"), (q_off, "q_off")):
+        if t.dtype != torch.int64:
+            raise TypeError(f"{name} must be int64")
+    if out is None:
+        out = torch.empty((max(n_r, 0), max(n_q, 0)), dtype=torch.float64, device=device)
+    ref_mz, ref_off = ref_mz.contiguous(), ref_off.contiguous()
+    q_mz, q_off = q_mz.contiguous(), q_off.contiguous()
+    err = torch.zeros(1, dtype=torch.int32, device=device) if check_errors else None
+    rc = lib.cms_intersect_mz(ptr(ref_mz), ptr(ref_off), n_r, int(ref_mz.shape[0]), ptr(q_mz),
+                              ptr(q_off), n_q, int(q_mz.shape[0]), float(scaling), ptr(out),
+                              int(out.stride(0)), ptr(err), stream_handle(s))
+    check(rc, "cms_intersect_mz")
+    if check_errors:
+        s.synchronize()
+        bits = int(err.item())
+        if bits:
+            _raise_device_error(bits, "cms_intersect_mz")
+    return out

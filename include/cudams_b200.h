@@ -383,6 +383,33 @@ int cms_fingerprint_symmetric(int measure, const uint32_t* ref_bits, const uint8
                               const uint32_t* q_bits, const uint8_t* q_valid, int64_t n,
                               int n_words, float fill, float* out, int64_t ld, void* stream);
 
+/*
+ * matchms ParentMassMatch / PrecursorMzMatch on the device (the reference
+ * prototypes both beside its CUDA classes: notebooks/prototyping/
+ * other_similarities.ipynb; matchms >= 0.24.0 is its requirement).  ref[i]
+ * and q[j] are the spectra's parent masses or precursor m/z (float64,
+ * device memory).  Writes out[i*ld + j] = 1 if
+ *   ppm == 0:  |ref[i] - q[j]| <= tolerance                   (Dalton)
+ *   ppm == 1:  |ref[i] - q[j]| / ((ref[i] + q[j]) / 2) * 1e6 <= tolerance
+ * in IEEE float64 in that order of operations, else 0 (NaN never matches).
+ */
+int cms_mass_match(const double* ref, int64_t n_ref, const double* q, int64_t n_q,
+                   double tolerance, int ppm, uint8_t* out, int64_t ld, void* stream);
+
+/*
+ * matchms IntersectMz on the device: for every (reference i, query j)
+ * out[i*ld + j] = scaling * |A & B| / |A | B| (float64, 0.0 when both sets
+ * are empty), A and B the sets of exact float64 m/z values of the two
+ * spectra (CSR: *_off[n+1] into *_mz, peaks sorted by m/z as matchms keeps
+ * them; repeated values count once).  Offsets outside [0, n_*_peaks] set
+ * bit 2 of *device_error (device memory, may be NULL) and the spectrum reads
+ * as empty.
+ */
+int cms_intersect_mz(const double* ref_mz, const int64_t* ref_off, int64_t n_ref,
+                     int64_t n_ref_peaks, const double* q_mz, const int64_t* q_off, int64_t n_q,
+                     int64_t n_q_peaks, double scaling, double* out, int64_t ld,
+                     uint32_t* device_error, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
