@@ -61,3 +61,36 @@ def test_no_cpu_fallback():
         pytest.skip("a GPU is present")
     with pytest.raises(_native.NativeError):
         _native.require_cuda()
+
+
+def test_metadata_entry_points_validate_without_gpu():
+    """cms_mass_match / cms_intersect_mz reject bad arguments before any CUDA
+    call, and empty problems succeed without one."""
+    from cudams import _native
+
+    lib = _native.load()
+    assert lib.cms_mass_match(None, 4, None, 4, 0.1, 2, None, 4, None) == _native.CMS_ERR_INVALID
+    assert "ppm" in _native.last_error()
+    assert lib.cms_mass_match(None, 4, None, 8, 0.1, 0, None, 4, None) == _native.CMS_ERR_INVALID
+    assert lib.cms_mass_match(None, 4, None, 4, 0.1, 0, None, 4, None) == _native.CMS_ERR_INVALID
+    assert "null pointer" in _native.last_error()
+    assert lib.cms_mass_match(None, 0, None, 4, 0.1, 0, None, 4, None) == _native.CMS_OK
+    rc = lib.cms_intersect_mz(None, None, 3, 10, None, None, 5, 10, 1.0, None, 4, None, None)
+    assert rc == _native.CMS_ERR_INVALID  # ld < n_q
+    rc = lib.cms_intersect_mz(None, None, 3, 10, None, None, 5, 10, 1.0, None, 5, None, None)
+    assert rc == _native.CMS_ERR_INVALID and "null pointer" in _native.last_error()
+    assert lib.cms_intersect_mz(None, None, 0, 0, None, None, 5, 0, 1.0, None, 5, None,
+                                None) == _native.CMS_OK
+
+
+def test_pack_mz64():
+    import numpy as np
+
+    from conftest import Spectrum
+    from cudams.similarity.CudaIntersectMz import pack_mz64
+
+    mz, off = pack_mz64([Spectrum([1.0, 2.0, 2.0], [1, 1, 1]), Spectrum([], []),
+                         Spectrum([0.5], [1])])
+    assert mz.dtype == np.float64 and off.dtype == np.int64
+    np.testing.assert_array_equal(off, [0, 3, 3, 4])
+    np.testing.assert_array_equal(mz, [1.0, 2.0, 2.0, 0.5])
